@@ -1,0 +1,69 @@
+"""Builds libftsp.so (the engine and its C ABI) in-tree for sm_100a.
+
+    python -m ftspolysol_b200.build [--force] [--verbose]
+
+The library is written next to this file (ftspolysol_b200/libftsp.so) so it
+travels with the source tree; nothing is installed into site-packages.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libftsp.so")
+
+SOURCES = ["engine.cu"]
+HEADERS = ["fft_core.cuh", "passes.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-O2",
+         "-Xptxas", "-warn-spills"]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else (shutil.which("nvcc") or "nvcc")
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "ftsp.h")]
+    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+
+
+def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    if not force and not _stale():
+        return LIB
+    cmd = [nvcc()] + ARCH + FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp"]
+    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    if extra:
+        cmd += list(extra)
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libftsp.so")
+    if verbose and (res.stdout or res.stderr):
+        print(res.stdout + res.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-info", action="store_true", help="print register/smem usage (-Xptxas -v)")
+    a = ap.parse_args()
+    build(force=a.force or a.ptxas_info, verbose=a.verbose or a.ptxas_info,
+          extra=["-Xptxas", "-v"] if a.ptxas_info else None)
+    print(LIB)

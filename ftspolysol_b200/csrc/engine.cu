@@ -1,0 +1,1695 @@
+// B200 complex-Langevin engine: device state, FFT executor, chain
+// propagators, densities, Langevin update and observables.
+//
+// One Engine<T> per system; T = double (FP64, reference-equivalent) or
+// float (complex64 fields and propagators, FP64 reductions).  All device
+// work of a handle is queued on one stream; a step needs no host
+// synchronisation except the final status read in ftsp_step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "passes.cuh"
+#include "ftsp.h"
+
+namespace ftsp {
+
+constexpr int MAXSP = 16;
+constexpr int MAXION = 16;
+constexpr int MAXM = 8;
+constexpr int MAXMODE = 8;
+constexpr int RED_BLOCKS = 296;   // fixed reduction grid (2 x 148 SMs) => deterministic sums
+constexpr int RED_THREADS = 256;
+constexpr double PI = 3.141592653589793238462643383279502884;
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+#define FTSP_CUDA(call)                                                                       \
+    do {                                                                                      \
+        cudaError_t err_ = (call);                                                            \
+        if (err_ != cudaSuccess)                                                              \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(err_));            \
+    } while (0)
+
+// ---- device scalars shared by the kernels of one step ----
+struct DevScal {
+    // every member is 16-byte aligned: several are read or written as double2
+    alignas(16) double2 Q[MAXSP];
+    alignas(16) double2 factor[MAXSP];
+    alignas(16) double2 Qion[MAXION];
+    alignas(16) double2 ion_factor[MAXION];
+    alignas(16) double2 mean_dpsi;
+    alignas(16) double2 mean_psi;
+    alignas(16) double mean_eta;
+    alignas(16) double corr[4];            // corrector: sum of psi (complex), non-finite cell count
+    alignas(16) double fsq[2 * MAXMODE];   // sum over the grid of omega_a^2 (complex)
+    alignas(16) double kobs[26];           // k-space observable sums
+    alignas(16) double dmax[MAXMODE + 1];
+    alignas(16) double rec[2 * 128];
+    alignas(16) int nonfinite;
+};
+static_assert(offsetof(DevScal, rec) % 16 == 0 && offsetof(DevScal, corr) % 16 == 0, "DevScal alignment");
+
+// ---- host configuration ----
+struct Cls {
+    int type;
+    double z;
+};
+
+struct Species {
+    double nc;
+    int N;
+    std::vector<int> type;
+    std::vector<double> charge, bond;
+    std::vector<int> cls;     // class of each segment
+    std::vector<int> bcls;    // bond-length class of each bond
+};
+
+struct Ion {
+    double z, count, smear;
+};
+
+struct HostCfg {
+    int m1, m2, m3;
+    size_t V;
+    double L[3];
+    double dV, a, lB, dt, lpsi, volume;
+    bool elec;
+    int M, nm;
+    std::vector<double> coeff, lambda, O;
+    std::vector<double2> gamma;
+    std::vector<Species> sp;
+    std::vector<Ion> ions;
+    std::vector<Cls> cls;
+    std::vector<double> bond_lengths;
+    double self_pressure;
+    int stress_mask, iso;
+    bool noise;
+    uint64_t seed;
+    int precision, scheme, device;
+    int n_stress() const { return __builtin_popcount(stress_mask); }
+    bool stress_on() const { return stress_mask != 0 || iso; }
+    int record_len() const
+    {
+        const int S = (int)sp.size(), J = (int)ions.size();
+        return 3 * (S + J) + 1 + n_stress() + (iso ? 1 : 0);
+    }
+};
+
+static FftPlan1 make_plan(int n)
+{
+    FftPlan1 p{};
+    p.n = n;
+    p.nst = 0;
+    int r = n;
+    while (r % 8 == 0 && r > 8) { p.rad[p.nst++] = 8; r /= 8; }
+    if (r == 8) { p.rad[p.nst++] = 8; r = 1; }
+    while (r % 4 == 0) { p.rad[p.nst++] = 4; r /= 4; }
+    while (r % 2 == 0) { p.rad[p.nst++] = 2; r /= 2; }
+    while (r % 3 == 0) { p.rad[p.nst++] = 3; r /= 3; }
+    while (r % 5 == 0) { p.rad[p.nst++] = 5; r /= 5; }
+    if (r != 1 || p.nst > 12) throw std::runtime_error("grid size " + std::to_string(n) + " is not 2/3/5-smooth");
+    return p;
+}
+
+static double wave_number(int i, int m, double L)
+{
+    const int mode = i > m / 2 ? i - m : i;
+    return 2.0 * PI * mode / L;
+}
+
+// ---------------------------------------------------------------------------
+// Generic kernels
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void k_foreach(size_t n, F f)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) f(i);
+}
+
+// Sum (MAX = false) or maximum (MAX = true) of K channels; partial[block*K + c].
+template <int K, bool MAX, class F>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* partial)
+{
+    __shared__ double scratch[(RED_THREADS / 32) * K];
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) f(i, acc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double x = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = MAX ? fmax(x, y) : x + y;
+        }
+        if (lane == 0) scratch[warp * K + c] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int w = 0; w < RED_THREADS / 32; ++w) {
+            const double y = scratch[w * K + threadIdx.x];
+            s = MAX ? fmax(s, y) : s + y;
+        }
+        partial[blockIdx.x * K + threadIdx.x] = s;
+    }
+}
+
+// Fixed-order combine of `count` partial rows of K channels.
+template <bool MAX>
+__global__ void k_combine(const double* partial, int count, int K, double* out)
+{
+    for (int c = threadIdx.x; c < K; c += blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < count; ++b) {
+            const double y = partial[(size_t)b * K + c];
+            s = MAX ? fmax(s, y) : s + y;
+        }
+        out[c] = s;
+    }
+}
+
+// ---- small complex helpers in double ----
+__device__ __forceinline__ double2 dmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 dinv(double2 z)  // Smith's algorithm, as common.h:146-157
+{
+    const double ax = fabs(z.x), ay = fabs(z.y);
+    if (ax >= ay) {
+        const double r = z.y / z.x, den = z.x * (1.0 + r * r);
+        return make_double2(1.0 / den, -r / den);
+    }
+    const double r = z.x / z.y, den = z.y * (1.0 + r * r);
+    return make_double2(r / den, -1.0 / den);
+}
+__device__ __forceinline__ double2 dneglog(double2 z)
+{
+    return make_double2(-log(sqrt(z.x * z.x + z.y * z.y)), -atan2(z.y, z.x));
+}
+template <typename V> __device__ __forceinline__ double2 to_d(V v) { return make_double2((double)v.x, (double)v.y); }
+template <typename V> __device__ __forceinline__ V from_d(double2 d)
+{
+    V v;
+    v.x = (typename RealOf<V>::type)d.x;
+    v.y = (typename RealOf<V>::type)d.y;
+    return v;
+}
+// exp of a complex number as common.h:188-192: r = exp(x); (r cos y, r sin y)
+__device__ __forceinline__ float2 cexpT(float x, float y)
+{
+    const float r = expf(x);
+    float s, c;
+    sincosf(y, &s, &c);
+    return make_float2(r * c, r * s);
+}
+__device__ __forceinline__ double2 cexpT(double x, double y)
+{
+    const double r = exp(x);
+    double s, c;
+    sincos(y, &s, &c);
+    return make_double2(r * c, r * s);
+}
+
+// ---- Philox4x32-10 counter-based generator (Salmon et al., SC'11) ----
+struct U4 {
+    uint32_t x, y, z, w;
+};
+__device__ __forceinline__ U4 philox(U4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    }
+    return c;
+}
+// One standard normal per (element, field, step) by the Box-Muller transform
+// of two 53-bit uniforms in (0, 1).
+__device__ __forceinline__ double normal_at(uint64_t seed, uint64_t step, uint32_t field, uint64_t i)
+{
+    const U4 r = philox(U4{(uint32_t)i, (uint32_t)(i >> 32), (uint32_t)step, field}, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double u1 = ((double)(((uint64_t)r.x << 21) ^ (r.y >> 11)) + 0.5) * (1.0 / 9007199254740992.0);
+    const double u2 = ((double)(((uint64_t)r.z << 21) ^ (r.w >> 11)) + 0.5) * (1.0 / 9007199254740992.0);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+// ---- plain-data tables captured by the kernels' lambdas ----
+struct GCoef {
+    double2 g[MAXMODE * MAXM];   // gamma_a O_{a alpha}
+};
+struct ModeTab {
+    double c[MAXMODE];
+    double s[MAXMODE];
+    double2 g[MAXMODE * MAXM];
+};
+struct SigTab {
+    double s[MAXMODE + 1];
+};
+struct ClsTab {
+    int type[64];
+    double z[64];
+};
+struct IonTab {
+    double z[MAXION];
+    double nd[MAXION];
+    double a2[MAXION];
+};
+struct ObsConst {
+    double2 g[MAXMODE * MAXM];
+    double z[MAXION];
+    double a2ion[MAXION];
+};
+struct RecConst {
+    double nv[MAXSP];
+    double self_poly[MAXSP];
+    double ideal_poly[MAXSP];
+    double nvion[MAXION];
+    double self_ion[MAXION];
+    double ideal_ion[MAXION];
+    double coeff[MAXMODE];
+    double ideal_stress[6];   // (ideal + self) delta + mode term
+    double ideal_iso;
+    int active[6];
+};
+
+// Loaders used by the plain transforms: field f of a batch reads src[f].
+template <typename T>
+struct OpLoadN {
+    const cplx<T>* s[16];
+    size_t fs;
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ cplx<T> operator()(int f, int, int, int, size_t g, cplx<T>) const { return s[f][g - f * fs]; }
+    __device__ __forceinline__ void end(double*, size_t) {}
+};
+template <typename T>
+struct OpLoadOne {
+    const cplx<T>* s;
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ cplx<T> operator()(int, int, int, int, size_t g, cplx<T>) const { return s[g]; }
+    __device__ __forceinline__ void end(double*, size_t) {}
+};
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+struct EngineBase {
+    HostCfg c;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    virtual ~EngineBase() {}
+    virtual void set_fields(const double* omega, const double* psi) = 0;
+    virtual long long get_field(const std::string& name, double* out) = 0;
+    virtual void compute_densities(int which, double* Q) = 0;
+    virtual void measure(int which, double* rec) = 0;
+    virtual void set_noise(const double* eta) = 0;
+    virtual int step(double* Qbar, double* rec, double* dmax, bool sync) = 0;
+    virtual int read_status(double* rec, double* dmax) = 0;
+    virtual void views(ftsp_views* v) = 0;
+};
+
+template <typename T>
+struct Buf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count)
+    {
+        n = count;
+        if (count) FTSP_CUDA(cudaMalloc(&p, sizeof(T) * count));
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+template <typename T>
+struct Engine : EngineBase {
+    using V = cplx<T>;
+    size_t V_ = 0;
+    bool plane_ok = false;
+    PlaneGeom pg{};
+    LineGeom gx{}, gy{}, gz{};
+    int plane_threads = 0, x_threads = 0, y_threads = 0, z_threads = 0;
+    size_t plane_smem = 0, x_smem = 0, y_smem = 0, z_smem = 0;
+    static constexpr int EP = sizeof(T) == 4 ? 32 : 16;   // elements per thread, plane pass
+    static constexpr int EL = 16;                          // elements per thread, line passes
+
+    // device buffers
+    Buf<V> tw1, tw2, tw3;
+    Buf<double> kx, ky, kz;
+    Buf<T> phi;          // per bond class: m1 + m2 + m3 separable factors
+    Buf<T> gam;          // Gamma of the beads, separable (m1 + m2 + m3)
+    Buf<T> gion;         // per ion: separable Gamma_j (m1 + m2 + m3)
+    Buf<V> omega, psi, omega_bar, psi_bar, drift, drift_bar, dpsi, dpsi_bar;
+    Buf<T> eta;          // (nm + 1) * V
+    Buf<V> kA;           // (nm + 1) * V : DFT of (omega_w, psi_w)
+    Buf<V> kB;           // (M + 1 + J) * V : W_type_s, psi_s, ion psi (real space)
+    Buf<V> dB;           // (M + 1 + J) * V : density accumulators + ion Boltzmann -> k-space
+    Buf<V> kC;           // (M + 3) * V : rho_type, rho_c_poly, rho_c_ion, psi-drift part
+    Buf<V> rho_p, rho_c, ion_rho;
+    Buf<V> E;            // class tables exp(-W_c)
+    Buf<V> qF, Fst, G, H;
+    Buf<double> part;    // reduction partials
+    Buf<double> spart;   // stress partials [ncta_x * 6] complex
+    DevScal* ds = nullptr;
+    DevScal hs{};
+    bool noise_injected = false;
+    uint64_t step_counter = 0;
+    int Nmax = 1;
+
+    explicit Engine(const HostCfg& cfg)
+    {
+        c = cfg;
+        FTSP_CUDA(cudaSetDevice(c.device));
+        V_ = c.V;
+        setup_geometry();
+        allocate();
+        build_tables();
+    }
+
+    ~Engine() override
+    {
+        Buf<V>* vb[] = {&tw1, &tw2, &tw3, &omega, &psi, &omega_bar, &psi_bar, &drift, &drift_bar, &dpsi, &dpsi_bar,
+                        &kA, &kB, &dB, &kC, &rho_p, &rho_c, &ion_rho, &E, &qF, &Fst, &G, &H};
+        for (auto* b : vb) b->release();
+        kx.release(); ky.release(); kz.release(); phi.release(); gam.release(); gion.release(); eta.release();
+        part.release(); spart.release();
+        if (ds) cudaFree(ds);
+    }
+
+    // ---- geometry and launch shapes ----
+    static int round32(int t) { return std::max(32, (t + 31) / 32 * 32); }
+
+    static int pick_W(int m3, int wmax)
+    {
+        int best = 1;
+        for (int w = 1; w <= std::min(m3, wmax); ++w)
+            if (m3 % w == 0) best = w;
+        return best;
+    }
+
+    template <class K>
+    void set_smem(K kernel, size_t bytes)
+    {
+        if (bytes > 48 * 1024) FTSP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    }
+
+    void setup_geometry()
+    {
+        const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
+        int dev_smem = 0;
+        FTSP_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+        pg.m1 = m1; pg.m2 = m2; pg.m3 = m3; pg.P = m3 + 1;
+        pg.py = make_plan(m2);
+        pg.pz = make_plan(m3);
+        plane_smem = sizeof(V) * ((size_t)m2 * pg.P + m2 + m3);
+        plane_smem = std::max(plane_smem, (size_t)32 * 16 * 8);
+        plane_threads = round32((m2 * m3 + EP - 1) / EP);
+        plane_ok = plane_smem <= (size_t)dev_smem && plane_threads <= 512;
+        const int wmax = std::max(1, std::min(sizeof(T) == 4 ? 32 : 16, (EL * 256) / std::max(m1, m2)));
+        const int W = pick_W(m3, wmax);
+        gx = LineGeom{m1, m2, m3, m1, W, 0, W, make_plan(m1)};
+        gy = LineGeom{m1, m2, m3, m2, W, 0, W, make_plan(m2)};
+        x_threads = round32((m1 * W + EL - 1) / EL);
+        y_threads = round32((m2 * W + EL - 1) / EL);
+        x_smem = std::max(sizeof(V) * ((size_t)m1 * W + m1), (size_t)32 * 16 * 8);
+        y_smem = std::max(sizeof(V) * ((size_t)m2 * W + m2), (size_t)32 * 16 * 8);
+        // z-lines: B rows with B*m3 ~ 2048 elements, B | m1*m2
+        if (m3 > EL * 256) throw std::runtime_error("z extent too large for the line passes");
+        int B = std::max(1, 2048 / m3);
+        while ((m1 * m2) % B) --B;
+        gz = LineGeom{m1, m2, m3, m3, 0, B, m3 + 1, make_plan(m3)};
+        z_threads = round32((B * m3 + EL - 1) / EL);
+        z_smem = std::max(sizeof(V) * ((size_t)B * (m3 + 1) + m3), (size_t)32 * 16 * 8);
+        if (x_threads > 256 || y_threads > 256 || z_threads > 256) throw std::runtime_error("grid dimension too large for the line passes");
+    }
+
+    void allocate()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, M = c.M, J = (int)c.ions.size();
+        tw1.alloc(c.m1); tw2.alloc(c.m2); tw3.alloc(c.m3);
+        kx.alloc(c.m1); ky.alloc(c.m2); kz.alloc(c.m3);
+        const int sum_m = c.m1 + c.m2 + c.m3;
+        phi.alloc((size_t)std::max<size_t>(1, c.bond_lengths.size()) * sum_m);
+        gam.alloc(sum_m);
+        gion.alloc((size_t)std::max(1, J) * sum_m);
+        const size_t nmv = Vn * std::max(1, nm);
+        omega.alloc(nmv); omega_bar.alloc(nmv); drift.alloc(nmv); drift_bar.alloc(nmv);
+        psi.alloc(Vn); psi_bar.alloc(Vn); dpsi.alloc(Vn); dpsi_bar.alloc(Vn);
+        eta.alloc((size_t)(nm + 1) * Vn);
+        kA.alloc((size_t)(nm + 1) * Vn);
+        kB.alloc((size_t)(M + 1 + J) * Vn);
+        dB.alloc((size_t)(M + 1 + J) * Vn);
+        kC.alloc((size_t)(M + 3) * Vn);
+        rho_p.alloc(Vn); rho_c.alloc(Vn); ion_rho.alloc(Vn * std::max(1, J));
+        E.alloc(Vn * std::max<size_t>(1, c.cls.size()));
+        Nmax = 1;
+        for (auto& s : c.sp) Nmax = std::max(Nmax, s.N);
+        qF.alloc(Vn * Nmax);
+        if (c.stress_on()) Fst.alloc(Vn * Nmax);
+        G.alloc(Vn); H.alloc(Vn);
+        part.alloc((size_t)std::max(RED_BLOCKS, std::max(c.m1, c.m1 * c.m2)) * 32);
+        spart.alloc((size_t)c.m2 * c.m3 * 12);
+        FTSP_CUDA(cudaMalloc(&ds, sizeof(DevScal)));
+        FTSP_CUDA(cudaMemset(ds, 0, sizeof(DevScal)));
+        FTSP_CUDA(cudaMemset(omega.p, 0, sizeof(V) * nmv));
+        FTSP_CUDA(cudaMemset(psi.p, 0, sizeof(V) * Vn));
+        FTSP_CUDA(cudaMemset(eta.p, 0, sizeof(T) * eta.n));
+    }
+
+    template <typename X>
+    void upload(Buf<X>& b, const std::vector<X>& h)
+    {
+        FTSP_CUDA(cudaMemcpy(b.p, h.data(), sizeof(X) * h.size(), cudaMemcpyHostToDevice));
+    }
+
+    void build_tables()
+    {
+        auto tw = [](int n) {
+            std::vector<V> t(n);
+            for (int j = 0; j < n; ++j) {
+                const long double ang = -2.0L * 3.141592653589793238462643383279502884L * j / n;
+                t[j].x = (T)cosl(ang);
+                t[j].y = (T)sinl(ang);
+            }
+            return t;
+        };
+        upload(tw1, tw(c.m1));
+        upload(tw2, tw(c.m2));
+        upload(tw3, tw(c.m3));
+        std::vector<double> hx(c.m1), hy(c.m2), hz(c.m3);
+        for (int i = 0; i < c.m1; ++i) hx[i] = wave_number(i, c.m1, c.L[0]);
+        for (int i = 0; i < c.m2; ++i) hy[i] = wave_number(i, c.m2, c.L[1]);
+        for (int i = 0; i < c.m3; ++i) hz[i] = wave_number(i, c.m3, c.L[2]);
+        upload(kx, hx); upload(ky, hy); upload(kz, hz);
+        // separable Gaussian factor tables exp(-f k_d^2) for each dimension
+        auto sep = [&](double f) {
+            std::vector<T> t;
+            for (double k : hx) t.push_back((T)std::exp(-f * k * k));
+            for (double k : hy) t.push_back((T)std::exp(-f * k * k));
+            for (double k : hz) t.push_back((T)std::exp(-f * k * k));
+            return t;
+        };
+        std::vector<T> ph;
+        for (double b : c.bond_lengths) {
+            auto t = sep(b * b / 6.0);
+            ph.insert(ph.end(), t.begin(), t.end());
+        }
+        if (ph.empty()) ph = sep(0.0);
+        upload(phi, ph);
+        upload(gam, sep(0.5 * c.a * c.a));
+        std::vector<T> gi;
+        for (auto& ion : c.ions) {
+            auto t = sep(0.5 * ion.smear * ion.smear);
+            gi.insert(gi.end(), t.begin(), t.end());
+        }
+        if (gi.empty()) gi = sep(0.0);
+        upload(gion, gi);
+    }
+
+    // ---- launch helpers ----
+    template <class F>
+    void foreach(size_t n, F f)
+    {
+        const int threads = 256;
+        const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 16);
+        k_foreach<<<std::max(1, blocks), threads, 0, stream>>>(n, f);
+        ++launches;
+    }
+
+    // Reduce K channels over n items into out[0..K) (device memory).
+    template <int K, bool MAX = false, class F>
+    void reduce(size_t n, F f, double* out)
+    {
+        k_reduce<K, MAX><<<RED_BLOCKS, RED_THREADS, 0, stream>>>(n, f, part.p);
+        k_combine<MAX><<<1, 64, 0, stream>>>(part.p, RED_BLOCKS, K, out);
+        launches += 2;
+    }
+
+    // Batched in-place (or out-of-place from per-field sources) 3-D FFT of nf
+    // contiguous fields of dst.  src[f] (optional) gives the input of field f.
+    template <int S>
+    void fft3(V* dst, int nf, const V* const* src = nullptr)
+    {
+        using OpLoad = OpLoadN<T>;
+        OpLoad in{};
+        for (int f = 0; f < nf && f < 16; ++f) in.s[f] = src ? src[f] : dst + (size_t)f * V_;
+        in.fs = V_;
+        OpLoad self{};
+        for (int f = 0; f < nf && f < 16; ++f) self.s[f] = dst + (size_t)f * V_;
+        self.fs = V_;
+        if (nf > 16) throw std::runtime_error("fft3: too many fields in one batch");
+        if (plane_ok) {
+            auto kp = k_plane<T, EP, 0, S, OpLoad>;
+            set_smem(kp, plane_smem);
+            kp<<<dim3(c.m1, nf), plane_threads, plane_smem, stream>>>(pg, nullptr, dst, V_, tw2.p, tw3.p, in);
+        } else {
+            auto kz = k_zline<T, EL, 0, S, OpLoad>;
+            set_smem(kz, z_smem);
+            kz<<<dim3(c.m1 * c.m2 / gz.B, nf), z_threads, z_smem, stream>>>(gz, nullptr, dst, V_, tw3.p, in);
+            auto ky_ = k_strided<T, EL, 1, 0, S, OpLoad>;
+            set_smem(ky_, y_smem);
+            ky_<<<dim3(c.m1 * (c.m3 / gy.W), nf), y_threads, y_smem, stream>>>(gy, nullptr, dst, V_, tw2.p, self);
+            ++launches;
+        }
+        auto kx_ = k_strided<T, EL, 0, 0, S, OpLoad>;
+        set_smem(kx_, x_smem);
+        kx_<<<dim3(c.m2 * (c.m3 / gx.W), nf), x_threads, x_smem, stream>>>(gx, nullptr, dst, V_, tw1.p, self);
+        launches += 2;
+    }
+
+    // Real-space pass of one segment: [inverse S1] op [forward S2] with the
+    // propagator op.  Plane pass when the plane fits, else y / z-line / y.
+    template <int S1, int S2, int KIND>
+    void seg_pass(const V* src, V* dst, const OpProp<T, KIND>& op)
+    {
+        using OpLoadOne = ftsp::OpLoadOne<T>;
+        if (plane_ok) {
+            auto kp = k_plane<T, EP, S1, S2, OpProp<T, KIND>>;
+            set_smem(kp, plane_smem);
+            kp<<<dim3(c.m1, 1), plane_threads, plane_smem, stream>>>(pg, src, dst, V_, tw2.p, tw3.p, op);
+            ++launches;
+            return;
+        }
+        if (S1 != 0) {   // y-lines of the inverse, in place on src
+            auto ky_ = k_strided<T, EL, 1, 0, S1, OpLoadOne>;
+            set_smem(ky_, y_smem);
+            ky_<<<dim3(c.m1 * (c.m3 / gy.W), 1), y_threads, y_smem, stream>>>(gy, nullptr, const_cast<V*>(src), V_, tw2.p, OpLoadOne{src});
+            ++launches;
+        }
+        auto kz_ = k_zline<T, EL, S1, S2, OpProp<T, KIND>>;
+        set_smem(kz_, z_smem);
+        kz_<<<dim3(c.m1 * c.m2 / gz.B, 1), z_threads, z_smem, stream>>>(gz, src, dst, V_, tw3.p, op);
+        ++launches;
+        if (S2 != 0) {   // y-lines of the forward transform, in place on dst
+            auto ky_ = k_strided<T, EL, 1, 0, S2, OpLoadOne>;
+            set_smem(ky_, y_smem);
+            ky_<<<dim3(c.m1 * (c.m3 / gy.W), 1), y_threads, y_smem, stream>>>(gy, nullptr, dst, V_, tw2.p, OpLoadOne{dst});
+            ++launches;
+        }
+    }
+
+    int seg_pass_ctas() const { return plane_ok ? c.m1 : c.m1 * c.m2 / gz.B; }
+    int x_ctas() const { return c.m2 * (c.m3 / gx.W); }
+
+    template <int S1, int S2, bool FWD, bool STRESS>
+    void bond_pass(const V* src, V* dst, const OpBond<T, FWD, STRESS>& op)
+    {
+        auto kx_ = k_strided<T, EL, 0, S1, S2, OpBond<T, FWD, STRESS>>;
+        set_smem(kx_, x_smem);
+        kx_<<<dim3(x_ctas(), 1), x_threads, x_smem, stream>>>(gx, src, dst, V_, tw1.p, op);
+        ++launches;
+    }
+
+    // ---- chain propagators of one species; densities accumulate into dB ----
+    void solve_species(int isp, bool stress)
+    {
+        const Species& s = c.sp[isp];
+        const int N = s.N;
+        const size_t Vn = V_;
+        const int M = c.M;
+        auto Ec = [&](int seg) { return E.p + (size_t)s.cls[seg] * Vn; };
+        auto qf = [&](int seg) { return qF.p + (size_t)seg * Vn; };
+        double2* factor = &ds->factor[isp];
+        double* qpart = part.p;
+        // ---- forward sweep ----
+        if (N == 1) {
+            OpProp<T, FWD_SINGLE> op{};
+            op.E = Ec(0); op.qstore = qf(0); op.partial = reinterpret_cast<double2*>(qpart);
+            seg_pass<0, 0, FWD_SINGLE>(nullptr, nullptr, op);
+        } else {
+            OpProp<T, FWD_START> op0{};
+            op0.E = Ec(0); op0.qstore = qf(0);
+            seg_pass<0, -1, FWD_START>(nullptr, G.p, op0);
+            for (int b = 0; b < N - 1; ++b) {
+                OpBond<T, true, false> ob{};
+                ob.Fstore = stress ? Fst.p + (size_t)b * Vn : nullptr;
+                set_bond(ob, s.bcls[b]);
+                bond_pass<-1, +1, true, false>(G.p, H.p, ob);
+                if (b + 1 < N - 1) {
+                    OpProp<T, FWD_MID> op{};
+                    op.E = Ec(b + 1); op.qstore = qf(b + 1);
+                    seg_pass<+1, -1, FWD_MID>(H.p, G.p, op);
+                } else {
+                    OpProp<T, FWD_LAST> op{};
+                    op.E = Ec(b + 1); op.qstore = qf(b + 1); op.partial = reinterpret_cast<double2*>(qpart);
+                    seg_pass<+1, 0, FWD_LAST>(H.p, nullptr, op);
+                }
+            }
+        }
+        // ---- Q and the species factor (n/V)/Q ----
+        {
+            const int cnt = seg_pass_ctas();
+            const double nv = s.nc / c.volume;
+            const double invV = 1.0 / (double)Vn;
+            DevScal* d = ds;
+            k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+                double sx = 0.0, sy = 0.0;
+                for (int i = 0; i < cnt; ++i) {
+                    sx += qpart[2 * i];
+                    sy += qpart[2 * i + 1];
+                }
+                const double2 Q = make_double2(sx * invV, sy * invV);
+                d->Q[isp] = Q;
+                d->factor[isp] = dscale(dinv(Q), nv);
+            });
+            ++launches;
+        }
+        // ---- backward sweep (opposite sign convention: B' = B(-k)) ----
+        auto rho_of = [&](int seg) { return dB.p + (size_t)s.type[seg] * Vn; };
+        auto rchg = [&](int seg) -> V* { return (c.elec && s.charge[seg] != 0.0) ? dB.p + (size_t)M * Vn : nullptr; };
+        if (N == 1) {
+            OpProp<T, BWD_SINGLE> op{};
+            op.qread = qf(0); op.rho_type = rho_of(0); op.rho_charge = rchg(0); op.z = (T)s.charge[0]; op.factor = factor;
+            seg_pass<0, 0, BWD_SINGLE>(nullptr, nullptr, op);
+            return;
+        }
+        {
+            OpProp<T, BWD_START> op{};
+            op.E = Ec(N - 1); op.qread = qf(N - 1); op.rho_type = rho_of(N - 1); op.rho_charge = rchg(N - 1);
+            op.z = (T)s.charge[N - 1]; op.factor = factor;
+            seg_pass<0, +1, BWD_START>(nullptr, G.p, op);
+        }
+        for (int b = N - 2; b >= 0; --b) {
+            if (stress) {
+                OpBond<T, false, true> ob{};
+                ob.Fread = Fst.p + (size_t)b * Vn;
+                ob.factor = factor;
+                ob.partial = reinterpret_cast<double2*>(spart.p);
+                ob.b2 = s.bond[b] * s.bond[b];
+                set_bond(ob, s.bcls[b]);
+                bond_pass<+1, -1, false, true>(G.p, H.p, ob);
+            } else {
+                OpBond<T, false, false> ob{};
+                set_bond(ob, s.bcls[b]);
+                bond_pass<+1, -1, false, false>(G.p, H.p, ob);
+            }
+            if (b > 0) {
+                OpProp<T, BWD_MID> op{};
+                op.E = Ec(b); op.qread = qf(b); op.rho_type = rho_of(b); op.rho_charge = rchg(b);
+                op.z = (T)s.charge[b]; op.factor = factor;
+                seg_pass<-1, +1, BWD_MID>(H.p, G.p, op);
+            } else {
+                OpProp<T, BWD_LAST> op{};
+                op.qread = qf(0); op.rho_type = rho_of(0); op.rho_charge = rchg(0);
+                op.z = (T)s.charge[0]; op.factor = factor;
+                seg_pass<-1, 0, BWD_LAST>(H.p, nullptr, op);
+            }
+        }
+    }
+
+    template <class OB>
+    void set_bond(OB& ob, int bc)
+    {
+        const int sum_m = c.m1 + c.m2 + c.m3;
+        const T* base = phi.p + (size_t)bc * sum_m;
+        ob.phix = base;
+        ob.phiy = base + c.m1;
+        ob.phiz = base + c.m1 + c.m2;
+        ob.kx = kx.p; ob.ky = ky.p; ob.kz = kz.p;
+        ob.invV = (T)(1.0 / (double)V_);
+    }
+
+    // ---- densities at (omega_w, psi_w) ----
+    void eval(int which, bool stress)
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, M = c.M, J = (int)c.ions.size();
+        const V* om = which ? omega_bar.p : omega.p;
+        const V* ps = which ? psi_bar.p : psi.p;
+        const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
+        const bool elec = c.elec;
+        // 1. DFT of the mode fields and psi
+        {
+            std::vector<const V*> src;
+            for (int a = 0; a < nm; ++a) src.push_back(om + (size_t)a * Vn);
+            src.push_back(ps);
+            fft3<-1>(kA.p, nm + 1, src.data());
+        }
+        // 2. k-space: W_type_s (M), psi_s, ion psi_j (J), all scaled by 1/V
+        {
+            GCoef co{};
+            for (int a = 0; a < nm; ++a)
+                for (int al = 0; al < M; ++al)
+                    co.g[a * M + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
+            const V* kAp = kA.p;
+            V* kBp = kB.p;
+            const T* gm = gam.p;
+            const T* gi = gion.p;
+            const int sum_m = m1 + m2 + m3;
+            const double invV = 1.0 / (double)Vn;
+            foreach(Vn, [=] __device__(size_t i) {
+                const int x = (int)(i / ((size_t)m2 * m3));
+                const int r = (int)(i - (size_t)x * m2 * m3);
+                const int y = r / m3, z = r - y * m3;
+                const T G0 = gm[x] * gm[m1 + y] * gm[m1 + m2 + z];
+                const double gv = (double)G0 * invV;
+                for (int al = 0; al < M; ++al) {
+                    double2 w = make_double2(0.0, 0.0);
+                    for (int a = 0; a < nm; ++a) w = dadd(w, dmul(to_d(kAp[(size_t)a * Vn + i]), co.g[a * M + al]));
+                    kBp[(size_t)al * Vn + i] = from_d<V>(dscale(w, gv));
+                }
+                const double2 P = to_d(kAp[(size_t)nm * Vn + i]);
+                kBp[(size_t)M * Vn + i] = from_d<V>(elec ? dscale(P, gv) : make_double2(0.0, 0.0));
+                for (int j = 0; j < J; ++j) {
+                    const T* t = gi + (size_t)j * sum_m;
+                    const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
+                    kBp[(size_t)(M + 1 + j) * Vn + i] = from_d<V>(elec ? dscale(P, gj) : make_double2(0.0, 0.0));
+                }
+            });
+        }
+        fft3<+1>(kB.p, M + 1 + J);
+        // 3. class tables exp(-(W_type + i z psi_s)), ion Boltzmann factors, zeroed accumulators
+        {
+            ClsTab ct{};
+            const int ncls = (int)c.cls.size();
+            if (ncls > 64) throw std::runtime_error("too many segment classes");
+            for (int k = 0; k < ncls; ++k) {
+                ct.type[k] = c.cls[k].type;
+                ct.z[k] = elec ? c.cls[k].z : 0.0;
+            }
+            IonTab zi{};
+            for (int j = 0; j < J; ++j) zi.z[j] = c.ions[j].z;
+            const V* kBp = kB.p;
+            V* Ep = E.p;
+            V* dBp = dB.p;
+            foreach(Vn, [=] __device__(size_t i) {
+                const V ps_ = kBp[(size_t)M * Vn + i];
+                for (int k = 0; k < ncls; ++k) {
+                    V w = kBp[(size_t)ct.type[k] * Vn + i];
+                    const T zz = (T)ct.z[k];
+                    if (zz != T(0)) {   // W += psi_s * (0 + i z)  (add_scaled_complex_const)
+                        w.x += -(ps_.y * zz);
+                        w.y += ps_.x * zz;
+                    }
+                    Ep[(size_t)k * Vn + i] = cexpT(-w.x, -w.y);
+                }
+                for (int al = 0; al <= M; ++al) dBp[(size_t)al * Vn + i] = mkc<V>(T(0), T(0));
+                for (int j = 0; j < J; ++j) {
+                    const V pj = kBp[(size_t)(M + 1 + j) * Vn + i];
+                    const T zz = (T)zi.z[j];
+                    dBp[(size_t)(M + 1 + j) * Vn + i] = cexpT(zz * pj.y, -zz * pj.x);
+                }
+            });
+        }
+        if (stress) FTSP_CUDA(cudaMemsetAsync(spart.p, 0, sizeof(double) * 12 * (size_t)x_ctas(), stream));
+        // 4. chain propagators of every species
+        for (int isp = 0; isp < (int)c.sp.size(); ++isp) solve_species(isp, stress);
+        // 5. DFT of the raw densities and the ion Boltzmann factors
+        fft3<-1>(dB.p, M + 1 + J);
+        // 6. ion partition functions from the DC bins
+        if (J > 0) {
+            DevScal* d = ds;
+            const V* dBp = dB.p;
+            IonTab ic{};
+            for (int j = 0; j < J; ++j) ic.nd[j] = c.ions[j].count / c.volume;
+            const double invV = 1.0 / (double)Vn;
+            k_foreach<<<1, 32, 0, stream>>>((size_t)J, [=] __device__(size_t j) {
+                const double2 Q = dscale(to_d(dBp[(size_t)(M + 1 + j) * Vn]), invV);
+                d->Qion[j] = Q;
+                d->ion_factor[j] = dscale(dinv(Q), ic.nd[j]);
+            });
+            ++launches;
+        }
+        // 7. k-space: smoothed densities, ion charge, psi drift part
+        {
+            const V* dBp = dB.p;
+            const V* kAp = kA.p;
+            V* kCp = kC.p;
+            const T* gm = gam.p;
+            const T* gi = gion.p;
+            const double* kxp = kx.p;
+            const double* kyp = ky.p;
+            const double* kzp = kz.p;
+            const int sum_m = m1 + m2 + m3;
+            const double invV = 1.0 / (double)Vn;
+            const double dpsi_scale = elec ? 1.0 / (4.0 * PI * c.lB) : 0.0;
+            IonTab zi{};
+            for (int j = 0; j < J; ++j) zi.z[j] = elec ? c.ions[j].z : 0.0;
+            const DevScal* d = ds;
+            foreach(Vn, [=] __device__(size_t i) {
+                const int x = (int)(i / ((size_t)m2 * m3));
+                const int r = (int)(i - (size_t)x * m2 * m3);
+                const int y = r / m3, z = r - y * m3;
+                const double gv = (double)(gm[x] * gm[m1 + y] * gm[m1 + m2 + z]) * invV;
+                for (int al = 0; al <= M; ++al) kCp[(size_t)al * Vn + i] = from_d<V>(dscale(to_d(dBp[(size_t)al * Vn + i]), gv));
+                double2 ci = make_double2(0.0, 0.0);
+                for (int j = 0; j < J; ++j) {
+                    const T* t = gi + (size_t)j * sum_m;
+                    const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
+                    const double2 f = d->ion_factor[j];
+                    ci = dadd(ci, dscale(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + i]), f), gj * zi.z[j]));
+                }
+                kCp[(size_t)(M + 1) * Vn + i] = from_d<V>(ci);
+                const double k2 = kxp[x] * kxp[x] + kyp[y] * kyp[y] + kzp[z] * kzp[z];
+                kCp[(size_t)(M + 2) * Vn + i] = from_d<V>(dscale(to_d(kAp[(size_t)nm * Vn + i]), k2 * invV * dpsi_scale));
+            });
+        }
+        fft3<+1>(kC.p, M + 3);
+        // 8. real-space epilogue: rho_p, rho_c, ion densities, raw psi drift (+ its sum)
+        {
+            const V* kCp = kC.p;
+            const V* kBp = kB.p;
+            V* rp = rho_p.p;
+            V* rc = rho_c.p;
+            V* ir = ion_rho.p;
+            V* dp = which ? dpsi_bar.p : dpsi.p;
+            const DevScal* d = ds;
+            IonTab iz{};
+            for (int j = 0; j < J; ++j) {
+                iz.z[j] = c.ions[j].z;
+                iz.nd[j] = c.ions[j].count / c.volume;
+            }
+            reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
+                V sum = mkc<V>(T(0), T(0));
+                for (int al = 0; al < M; ++al) sum = cadd(sum, kCp[(size_t)al * Vn + i]);
+                rp[i] = sum;
+                const V rcp = kCp[(size_t)M * Vn + i];
+                const V rci = kCp[(size_t)(M + 1) * Vn + i];
+                const V rcv = elec ? cadd(rcp, rci) : mkc<V>(T(0), T(0));
+                rc[i] = rcv;
+                for (int j = 0; j < J; ++j) {
+                    if (elec) {
+                        const V pj = kBp[(size_t)(M + 1 + j) * Vn + i];
+                        const T zz = (T)iz.z[j];
+                        const V b = cexpT(zz * pj.y, -zz * pj.x);
+                        ir[(size_t)j * Vn + i] = cmul(b, from_d<V>(d->ion_factor[j]));
+                    } else {
+                        ir[(size_t)j * Vn + i] = mkc<V>((T)iz.nd[j], T(0));
+                    }
+                }
+                V dv = kCp[(size_t)(M + 2) * Vn + i];
+                if (elec) {
+                    dv.x -= rcv.y;   // + i * rho_c
+                    dv.y += rcv.x;
+                } else {
+                    dv = mkc<V>(T(0), T(0));
+                }
+                dp[i] = dv;
+                acc[0] += (double)dv.x;
+                acc[1] += (double)dv.y;
+            }, reinterpret_cast<double*>(&ds->mean_dpsi));
+        }
+        // when electrostatics are off the charge fields stay zero
+        if (!elec) {
+            FTSP_CUDA(cudaMemsetAsync(kC.p + (size_t)M * Vn, 0, sizeof(V) * 2 * Vn, stream));
+        }
+    }
+
+    // ---- drifts u_a = c_a w_a + sum_alpha gamma_a O_{a alpha} rho_alpha (+ sum of w^2) ----
+    void drifts(int which)
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, M = c.M;
+        const V* om = which ? omega_bar.p : omega.p;
+        V* u = which ? drift_bar.p : drift.p;
+        const V* rt = kC.p;
+        ModeTab co{};
+        for (int a = 0; a < nm; ++a) {
+            co.c[a] = c.coeff[a];
+            for (int al = 0; al < M; ++al)
+                co.g[a * M + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
+        }
+        reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
+            for (int a = 0; a < nm; ++a) {
+                const V w = om[(size_t)a * Vn + i];
+                // clear, add_scaled_complex(w, c), add_scaled_complex_const(rho, gamma O)
+                V v = cscale(w, (T)co.c[a]);
+                for (int al = 0; al < M; ++al) v = cadd(v, cmul(rt[(size_t)al * Vn + i], from_d<V>(co.g[a * M + al])));
+                u[(size_t)a * Vn + i] = v;
+                const double2 wd = to_d(w);
+                acc[2 * a] += wd.x * wd.x - wd.y * wd.y;
+                acc[2 * a + 1] += 2.0 * wd.x * wd.y;
+            }
+        }, ds->fsq);
+    }
+
+    // ---- noise for this step (generated, or injected by ftsp_set_noise) ----
+    void noises()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        T* e = eta.p;
+        if (!noise_injected) {
+            SigTab sg{};
+            for (int a = 0; a < nm; ++a) sg.s[a] = c.noise ? std::sqrt(2.0 * c.lambda[a] * c.dt / c.dV) : 0.0;
+            sg.s[nm] = (c.elec && c.noise) ? std::sqrt(2.0 * c.lpsi * c.dt / c.dV) : 0.0;
+            const uint64_t seed = c.seed, st = step_counter;
+            foreach(Vn, [=] __device__(size_t i) {
+                for (int f = 0; f <= nm; ++f)
+                    e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)(sg.s[f] * normal_at(seed, st, (uint32_t)f, i)) : T(0);
+            });
+        }
+        noise_injected = false;
+        if (c.elec) {   // remove_real_mean of the psi noise (complexLangevin.cu:296)
+            const T* ep = e + (size_t)nm * Vn;
+            reduce<1>(Vn, [=] __device__(size_t i, double* acc) { acc[0] += (double)ep[i]; }, &ds->mean_eta);
+        }
+    }
+
+    // ---- predictor (complexLangevin.cu:328-347) ----
+    void predictor()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        ModeTab co{};
+        for (int a = 0; a < nm; ++a) co.s[a] = -c.dt * c.lambda[a];
+        const double sp = -c.dt * c.lpsi;
+        const bool elec = c.elec;
+        const V* om = omega.p;
+        const V* u = drift.p;
+        V* ob = omega_bar.p;
+        const V* ps = psi.p;
+        V* pb = psi_bar.p;
+        V* dp = dpsi.p;
+        T* e = eta.p;
+        DevScal* d = ds;
+        const double invV = 1.0 / (double)Vn;
+        reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
+            const double me = elec ? d->mean_eta * invV : 0.0;
+            T ep = e[(size_t)nm * Vn + i];
+            if (elec) {
+                ep = (T)((double)ep + (-me));
+                e[(size_t)nm * Vn + i] = ep;
+            }
+            for (int a = 0; a < nm; ++a) {
+                V v = om[(size_t)a * Vn + i];
+                v = cadd(v, cscale(u[(size_t)a * Vn + i], (T)co.s[a]));
+                v.x += e[(size_t)a * Vn + i];
+                ob[(size_t)a * Vn + i] = v;
+            }
+            V pv = mkc<V>(T(0), T(0));
+            if (elec) {
+                const double2 md = dscale(d->mean_dpsi, -invV);
+                V dv = dp[i];
+                dv = cadd(dv, from_d<V>(md));
+                dp[i] = dv;
+                pv = cadd(ps[i], cscale(dv, (T)sp));
+                pv.x += ep;
+            }
+            pb[i] = pv;
+            acc[0] += (double)pv.x;
+            acc[1] += (double)pv.y;
+        }, reinterpret_cast<double*>(&ds->mean_psi));
+        remove_mean(psi_bar.p, &ds->mean_psi);
+    }
+
+    // f -= (sum / V), the sum being a device-side complex value
+    void remove_mean(V* f, const double2* sum)
+    {
+        if (!c.elec) return;
+        const double invV = 1.0 / (double)V_;
+        foreach(V_, [=] __device__(size_t i) {
+            const double2 m = dscale(*sum, -invV);
+            f[i] = cadd(f[i], from_d<V>(m));
+        });
+    }
+
+    // ---- corrector (complexLangevin.cu:349-368) + drift maxima + finite flag ----
+    void corrector()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        ModeTab co{};
+        for (int a = 0; a < nm; ++a) co.s[a] = -0.5 * c.dt * c.lambda[a];
+        const double sp = -0.5 * c.dt * c.lpsi;
+        const bool elec = c.elec;
+        V* om = omega.p;
+        const V* u0 = drift.p;
+        const V* u1 = drift_bar.p;
+        V* ps = psi.p;
+        const V* dp = dpsi.p;
+        V* db = dpsi_bar.p;
+        const T* e = eta.p;
+        DevScal* d = ds;
+        const double invV = 1.0 / (double)Vn;
+        // drift maxima: max |u + u_bar|^2 per mode and for psi
+        reduce<MAXMODE + 1, true>(Vn, [=] __device__(size_t i, double* acc) {
+            for (int a = 0; a < nm; ++a) {
+                const V s = cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]);
+                double v = (double)s.x * s.x + (double)s.y * s.y;
+                if (!isfinite(v)) v = INFINITY;
+                acc[a] = fmax(acc[a], v);
+            }
+            V dbv = db[i];
+            if (elec) dbv = cadd(dbv, from_d<V>(dscale(d->mean_dpsi, -invV)));
+            const V s = cadd(dp[i], dbv);
+            double v = (double)s.x * s.x + (double)s.y * s.y;
+            if (!isfinite(v)) v = INFINITY;
+            acc[nm] = fmax(acc[nm], v);
+        }, ds->dmax);
+        reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
+            bool bad = false;
+            for (int a = 0; a < nm; ++a) {
+                V w = om[(size_t)a * Vn + i];
+                w = cadd(w, cscale(u0[(size_t)a * Vn + i], (T)co.s[a]));
+                w = cadd(w, cscale(u1[(size_t)a * Vn + i], (T)co.s[a]));
+                w.x += e[(size_t)a * Vn + i];
+                om[(size_t)a * Vn + i] = w;
+                bad |= !(isfinite((double)w.x) && isfinite((double)w.y));
+            }
+            V pv = ps[i];
+            if (elec) {
+                V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+                db[i] = dbv;
+                pv = cadd(pv, cscale(dp[i], (T)sp));
+                pv = cadd(pv, cscale(dbv, (T)sp));
+                pv.x += e[(size_t)nm * Vn + i];
+            } else {
+                pv = mkc<V>(T(0), T(0));
+            }
+            ps[i] = pv;
+            acc[0] += (double)pv.x;
+            acc[1] += (double)pv.y;
+            if (bad || !(isfinite((double)pv.x) && isfinite((double)pv.y))) acc[2] += 1.0;
+        }, ds->corr);
+        remove_mean(psi.p, reinterpret_cast<const double2*>(ds->corr));
+    }
+
+    // ---- observables from k-space sums (Parseval) ----
+    void kspace_obs()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, M = c.M, J = (int)c.ions.size();
+        const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
+        const bool elec = c.elec;
+        ObsConst oc{};
+        for (int a = 0; a < nm; ++a)
+            for (int al = 0; al < M; ++al)
+                oc.g[a * M + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
+        for (int j = 0; j < J; ++j) {
+            oc.z[j] = c.ions[j].z;
+            oc.a2ion[j] = c.ions[j].smear * c.ions[j].smear;
+        }
+        const double a2 = c.a * c.a;
+        const V* kAp = kA.p;
+        const V* dBp = dB.p;
+        const T* gm = gam.p;
+        const T* gi = gion.p;
+        const double* kxp = kx.p;
+        const double* kyp = ky.p;
+        const double* kzp = kz.p;
+        const int sum_m = m1 + m2 + m3;
+        const DevScal* d = ds;
+        reduce<26>(Vn, [=] __device__(size_t i, double* acc) {
+            const int x = (int)(i / ((size_t)m2 * m3));
+            const int r = (int)(i - (size_t)x * m2 * m3);
+            const int y = r / m3, z = r - y * m3;
+            const int nx = x ? m1 - x : 0, ny = y ? m2 - y : 0, nz = z ? m3 - z : 0;
+            const size_t ineg = ((size_t)nx * m2 + ny) * m3 + nz;
+            const double ax = kxp[x], ay = kyp[y], az = kzp[z];
+            const double kk[6] = {ax * ax, ay * ay, az * az, ax * ay, ax * az, ay * az};
+            const double Gk = (double)(gm[x] * gm[m1 + y] * gm[m1 + m2 + z]);
+            // A = sum_alpha R_alpha(-k) W_alpha(k),  W_alpha = Gamma sum_a g_{a alpha} Omega_a
+            double2 A = make_double2(0.0, 0.0);
+            for (int al = 0; al < M; ++al) {
+                double2 w = make_double2(0.0, 0.0);
+                for (int a = 0; a < nm; ++a) w = dadd(w, dmul(to_d(kAp[(size_t)a * Vn + i]), oc.g[a * M + al]));
+                A = dadd(A, dmul(to_d(dBp[(size_t)al * Vn + ineg]), dscale(w, Gk)));
+            }
+            double2 Bc = make_double2(0.0, 0.0), Ij = make_double2(0.0, 0.0), I0 = make_double2(0.0, 0.0), X = make_double2(0.0, 0.0);
+            if (elec) {
+                const double2 Pk = to_d(kAp[(size_t)nm * Vn + i]);
+                const double2 Pm = to_d(kAp[(size_t)nm * Vn + ineg]);
+                const double2 rc = dmul(to_d(dBp[(size_t)M * Vn + ineg]), dscale(Pk, Gk));
+                Bc = make_double2(-rc.y, rc.x);   // i * R_c(-k) Gamma Psi(k)
+                for (int j = 0; j < J; ++j) {
+                    const T* t = gi + (size_t)j * sum_m;
+                    const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]);
+                    const double2 p = dmul(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + ineg]), d->ion_factor[j]), dscale(Pk, gj * oc.z[j]));
+                    const double2 ip = make_double2(-p.y, p.x);
+                    Ij = dadd(Ij, dscale(ip, -oc.a2ion[j]));
+                    I0 = dadd(I0, dscale(ip, 1.0 / 6.0));
+                }
+                X = dmul(Pk, Pm);
+            }
+            const double2 base = make_double2(-a2 * (A.x + Bc.x) + Ij.x, -a2 * (A.y + Bc.y) + Ij.y);
+            for (int cc = 0; cc < 6; ++cc) {
+                acc[2 * cc] += kk[cc] * base.x;
+                acc[2 * cc + 1] += kk[cc] * base.y;
+                acc[14 + 2 * cc] += kk[cc] * X.x;
+                acc[14 + 2 * cc + 1] += kk[cc] * X.y;
+            }
+            acc[12] += 0.5 * A.x + Bc.x / 6.0 + I0.x;
+            acc[13] += 0.5 * A.y + Bc.y / 6.0 + I0.y;
+        }, ds->kobs);
+    }
+
+    void finalize_record(bool with_stress)
+    {
+        const int S = (int)c.sp.size(), J = (int)c.ions.size(), nm = c.nm;
+        RecConst rc{};
+        for (int s = 0; s < S; ++s) {
+            double zz = 0.0;
+            for (double q : c.sp[s].charge) zz += q * q;
+            rc.nv[s] = c.sp[s].nc / c.volume;
+            rc.self_poly[s] = -c.lB * zz / (2.0 * std::sqrt(PI) * c.a);
+            rc.ideal_poly[s] = std::log(c.sp[s].nc / c.volume);
+        }
+        double ion_total = 0.0;
+        for (int j = 0; j < J; ++j) {
+            rc.nvion[j] = c.ions[j].count / c.volume;
+            rc.self_ion[j] = -c.lB * c.ions[j].z * c.ions[j].z / (2.0 * std::sqrt(PI) * c.ions[j].smear);
+            rc.ideal_ion[j] = std::log(c.ions[j].count / c.volume);
+            ion_total += c.ions[j].count;
+        }
+        for (int a = 0; a < nm; ++a) rc.coeff[a] = c.coeff[a];
+        double chains = 0.0;
+        for (auto& s : c.sp) chains += s.nc;
+        const double ideal = (chains + ion_total) / c.volume;
+        // mode term of stress::build_kernels (stress.cu:106-149)
+        double sum[6] = {0, 0, 0, 0, 0, 0};
+        long long modes = 0;
+        if (c.elec) {
+            std::vector<double> hx(c.m1), hy(c.m2), hz(c.m3);
+            for (int i = 0; i < c.m1; ++i) hx[i] = wave_number(i, c.m1, c.L[0]);
+            for (int i = 0; i < c.m2; ++i) hy[i] = wave_number(i, c.m2, c.L[1]);
+            for (int i = 0; i < c.m3; ++i) hz[i] = wave_number(i, c.m3, c.L[2]);
+            for (int x = 0; x < c.m1; ++x)
+                for (int y = 0; y < c.m2; ++y)
+                    for (int z = 0; z < c.m3; ++z) {
+                        const double k2 = hx[x] * hx[x] + hy[y] * hy[y] + hz[z] * hz[z];
+                        if (k2 > 0.0) {
+                            ++modes;
+                            const double v[6] = {hx[x] * hx[x], hy[y] * hy[y], hz[z] * hz[z], hx[x] * hy[y], hx[x] * hz[z], hy[y] * hz[z]};
+                            for (int cc = 0; cc < 6; ++cc) sum[cc] += v[cc] / k2;
+                        }
+                    }
+        }
+        for (int cc = 0; cc < 6; ++cc) {
+            const double delta = cc < 3 ? 1.0 : 0.0;
+            const double mode_term = c.elec ? ((1.0 / 3.0) * (double)modes * delta - sum[cc]) / c.volume : 0.0;
+            rc.ideal_stress[cc] = (ideal + c.self_pressure) * delta + mode_term;
+        }
+        rc.ideal_iso = ideal + c.self_pressure;
+        int na = 0;
+        for (int cc = 0; cc < 6; ++cc)
+            if (c.stress_mask & (1 << cc)) rc.active[na++] = cc;
+        const int iso = c.iso;
+        const double V2 = (double)V_ * (double)V_;
+        const double invV = 1.0 / (double)V_;
+        const double lB = c.lB;
+        const bool elec = c.elec;
+        const int nx = x_ctas();
+        const double* sp = spart.p;
+        DevScal* d = ds;
+        const bool ws = with_stress;
+        k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+            double2* rec = reinterpret_cast<double2*>(d->rec);
+            int k = 0;
+            double2 chem[MAXSP + MAXION];
+            for (int s = 0; s < S; ++s) chem[s] = dneglog(d->Q[s]);
+            for (int j = 0; j < J; ++j) chem[S + j] = elec ? dneglog(d->Qion[j]) : make_double2(0.0, 0.0);
+            for (int i = 0; i < S + J; ++i) rec[k++] = chem[i];
+            for (int s = 0; s < S; ++s) rec[k++] = make_double2(rc.self_poly[s], 0.0);
+            for (int j = 0; j < J; ++j) rec[k++] = make_double2(rc.self_ion[j], 0.0);
+            for (int s = 0; s < S; ++s) rec[k++] = make_double2(rc.ideal_poly[s], 0.0);
+            for (int j = 0; j < J; ++j) rec[k++] = make_double2(rc.ideal_ion[j], 0.0);
+            double2 Hm = make_double2(0.0, 0.0);
+            for (int a = 0; a < nm; ++a) Hm = dadd(Hm, make_double2(0.5 * rc.coeff[a] * d->fsq[2 * a] * invV, 0.5 * rc.coeff[a] * d->fsq[2 * a + 1] * invV));
+            const double* ko = d->kobs;
+            const double2 Xtr = make_double2(ko[14] + ko[16] + ko[18], ko[15] + ko[17] + ko[19]);
+            if (elec) Hm = dadd(Hm, dscale(Xtr, 1.0 / (8.0 * PI * lB * V2)));
+            for (int s = 0; s < S; ++s) Hm = dadd(Hm, dscale(chem[s], rc.nv[s]));
+            for (int j = 0; j < J; ++j) Hm = dadd(Hm, dscale(chem[S + j], rc.nvion[j]));
+            rec[k++] = Hm;
+            if (ws) {
+                // connectivity sums over the bond-pass CTAs
+                double2 Sc[6];
+                for (int cc = 0; cc < 6; ++cc) {
+                    double sx = 0.0, sy = 0.0;
+                    for (int b = 0; b < nx; ++b) {
+                        sx += sp[(size_t)b * 12 + 2 * cc];
+                        sy += sp[(size_t)b * 12 + 2 * cc + 1];
+                    }
+                    Sc[cc] = make_double2(sx, sy);
+                }
+                const double2 V0 = make_double2(ko[12], ko[13]);
+                for (int q = 0; q < na; ++q) {
+                    const int cc = rc.active[q];
+                    const double delta = cc < 3 ? 1.0 : 0.0;
+                    double2 v = make_double2(rc.ideal_stress[cc], 0.0);
+                    if (elec) {
+                        const double2 e = make_double2(ko[14 + 2 * cc] - delta * Xtr.x / 3.0, ko[14 + 2 * cc + 1] - delta * Xtr.y / 3.0);
+                        v = dadd(v, dscale(e, 1.0 / (4.0 * PI * lB * V2)));
+                    }
+                    v = dadd(v, dscale(Sc[cc], 1.0 / (3.0 * V2)));
+                    v = dadd(v, dscale(make_double2(ko[2 * cc] + delta * V0.x, ko[2 * cc + 1] + delta * V0.y), 1.0 / V2));
+                    rec[k++] = v;
+                }
+                if (iso) {
+                    double2 v = make_double2(rc.ideal_iso, 0.0);
+                    v = dadd(v, dscale(dadd(dadd(Sc[0], Sc[1]), Sc[2]), 1.0 / (9.0 * V2)));
+                    const double2 tr = make_double2((ko[0] + ko[2] + ko[4]) / 3.0 + V0.x, (ko[1] + ko[3] + ko[5]) / 3.0 + V0.y);
+                    v = dadd(v, dscale(tr, 1.0 / V2));
+                    rec[k++] = v;
+                }
+            }
+        });
+        ++launches;
+    }
+
+    // ---- API ----
+    void to_device_field(V* dst, const double* src, size_t count)
+    {
+        if (sizeof(T) == 8) {
+            FTSP_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * 2 * count, cudaMemcpyHostToDevice, stream));
+        } else {
+            std::vector<V> tmp(count);
+            for (size_t i = 0; i < count; ++i) {
+                tmp[i].x = (T)src[2 * i];
+                tmp[i].y = (T)src[2 * i + 1];
+            }
+            FTSP_CUDA(cudaMemcpyAsync(dst, tmp.data(), sizeof(V) * count, cudaMemcpyHostToDevice, stream));
+            FTSP_CUDA(cudaStreamSynchronize(stream));
+        }
+    }
+
+    void set_fields(const double* om, const double* ps) override
+    {
+        if (c.nm > 0) to_device_field(omega.p, om, (size_t)c.nm * V_);
+        to_device_field(psi.p, ps, V_);
+        if (c.elec) {
+            const V* p = psi.p;
+            reduce<2>(V_, [=] __device__(size_t i, double* acc) {
+                acc[0] += (double)p[i].x;
+                acc[1] += (double)p[i].y;
+            }, reinterpret_cast<double*>(&ds->mean_psi));
+            remove_mean(psi.p, &ds->mean_psi);
+        } else {
+            FTSP_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(V) * V_, stream));
+        }
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    long long get_field(const std::string& name, double* out) override
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, M = c.M, J = (int)c.ions.size();
+        const V* p = nullptr;
+        size_t n = 0;
+        if (name == "omega") { p = omega.p; n = nm * Vn; }
+        else if (name == "psi") { p = psi.p; n = Vn; }
+        else if (name == "omega_bar") { p = omega_bar.p; n = nm * Vn; }
+        else if (name == "psi_bar") { p = psi_bar.p; n = Vn; }
+        else if (name == "drift") { p = drift.p; n = nm * Vn; }
+        else if (name == "drift_bar") { p = drift_bar.p; n = nm * Vn; }
+        else if (name == "dpsi") { p = dpsi.p; n = Vn; }
+        else if (name == "dpsi_bar") { p = dpsi_bar.p; n = Vn; }
+        else if (name == "rho_type") { p = kC.p; n = (size_t)M * Vn; }
+        else if (name == "rho_c_poly") { p = kC.p + (size_t)M * Vn; n = Vn; }
+        else if (name == "rho_c_ion") { p = kC.p + (size_t)(M + 1) * Vn; n = Vn; }
+        else if (name == "rho_p") { p = rho_p.p; n = Vn; }
+        else if (name == "rho_c") { p = rho_c.p; n = Vn; }
+        else if (name == "ion_rho") { p = ion_rho.p; n = (size_t)J * Vn; }
+        else if (name == "W_type_s") { p = kB.p; n = (size_t)M * Vn; }
+        else if (name == "psi_s") { p = kB.p + (size_t)M * Vn; n = Vn; }
+        else if (name == "qF") { p = qF.p; n = (size_t)Nmax * Vn; }
+        else return -1;
+        if (out && n) {
+            std::vector<V> tmp(n);
+            FTSP_CUDA(cudaMemcpyAsync(tmp.data(), p, sizeof(V) * n, cudaMemcpyDeviceToHost, stream));
+            FTSP_CUDA(cudaStreamSynchronize(stream));
+            for (size_t i = 0; i < n; ++i) {
+                out[2 * i] = (double)tmp[i].x;
+                out[2 * i + 1] = (double)tmp[i].y;
+            }
+        }
+        return (long long)(2 * n);
+    }
+
+    void pull_scalars()
+    {
+        FTSP_CUDA(cudaMemcpyAsync(&hs, ds, sizeof(DevScal), cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void compute_densities(int which, double* Q) override
+    {
+        eval(which, false);
+        pull_scalars();
+        if (Q)
+            for (size_t s = 0; s < c.sp.size(); ++s) {
+                Q[2 * s] = hs.Q[s].x;
+                Q[2 * s + 1] = hs.Q[s].y;
+            }
+    }
+
+    void field_squares(int which)
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        const V* om = which ? omega_bar.p : omega.p;
+        reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
+            for (int a = 0; a < nm; ++a) {
+                const double2 wd = to_d(om[(size_t)a * Vn + i]);
+                acc[2 * a] += wd.x * wd.x - wd.y * wd.y;
+                acc[2 * a + 1] += 2.0 * wd.x * wd.y;
+            }
+        }, ds->fsq);
+    }
+
+    void measure(int which, double* rec) override
+    {
+        const bool st = c.stress_on();
+        eval(which, st);
+        field_squares(which);
+        kspace_obs();
+        finalize_record(st);
+        pull_scalars();
+        if (rec) std::memcpy(rec, hs.rec, sizeof(double) * 2 * c.record_len());
+    }
+
+    void set_noise(const double* e) override
+    {
+        const size_t n = (size_t)(c.nm + 1) * V_;
+        std::vector<T> tmp(n);
+        for (size_t i = 0; i < n; ++i) tmp[i] = (T)e[i];
+        FTSP_CUDA(cudaMemcpyAsync(eta.p, tmp.data(), sizeof(T) * n, cudaMemcpyHostToDevice, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        noise_injected = true;
+    }
+
+    void step_device()
+    {
+        const bool st = c.stress_on();
+        eval(0, false);
+        // save Q of the first evaluation for the finite check
+        FTSP_CUDA(cudaMemsetAsync(&ds->nonfinite, 0, sizeof(int), stream));
+        {
+            DevScal* d = ds;
+            const int S = (int)c.sp.size();
+            k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+                for (int s = 0; s < S; ++s)
+                    if (!isfinite(d->Q[s].x) || !isfinite(d->Q[s].y)) d->nonfinite = 1;
+            });
+            ++launches;
+        }
+        noises();
+        drifts(0);
+        predictor();
+        eval(1, st);
+        drifts(1);
+        kspace_obs();
+        finalize_record(st);
+        corrector();
+        ++step_counter;
+    }
+
+    int status_from_host()
+    {
+        const int S = (int)c.sp.size();
+        bool bad = hs.nonfinite != 0;
+        for (int s = 0; s < S; ++s) bad |= !(std::isfinite(hs.Q[s].x) && std::isfinite(hs.Q[s].y));
+        for (int i = 0; i < 2 * c.record_len(); ++i) bad |= !std::isfinite(hs.rec[i]);
+        // the corrector's third reduction channel counts non-finite cells
+        return bad ? FTSP_NONFINITE : FTSP_OK;
+    }
+
+    int step(double* Qbar, double* rec, double* dmax, bool sync) override
+    {
+        launches = 0;
+        step_device();
+        if (!sync) return FTSP_OK;
+        return read_status_impl(Qbar, rec, dmax);
+    }
+
+    int read_status_impl(double* Qbar, double* rec, double* dmax)
+    {
+        pull_scalars();
+        if (Qbar)
+            for (size_t s = 0; s < c.sp.size(); ++s) {
+                Qbar[2 * s] = hs.Q[s].x;
+                Qbar[2 * s + 1] = hs.Q[s].y;
+            }
+        if (rec) std::memcpy(rec, hs.rec, sizeof(double) * 2 * c.record_len());
+        if (dmax) {
+            for (int a = 0; a < c.nm; ++a) dmax[a] = std::fabs(0.5 * c.lambda[a]) * std::sqrt(std::max(0.0, hs.dmax[a]));
+            dmax[c.nm] = std::fabs(0.5 * c.lpsi) * std::sqrt(std::max(0.0, hs.dmax[c.nm]));
+        }
+        int st = status_from_host();
+        if (hs.corr[2] != 0.0) st = FTSP_NONFINITE;
+        return st;
+    }
+
+    int read_status(double* rec, double* dmax) override { return read_status_impl(nullptr, rec, dmax); }
+
+    void views(ftsp_views* v) override
+    {
+        if (sizeof(T) != 8) throw std::runtime_error("state views are available for FP64 handles only");
+        const size_t Vn = V_;
+        v->omega = omega.p; v->psi = psi.p; v->omega_bar = omega_bar.p; v->psi_bar = psi_bar.p;
+        v->rho_type = kC.p; v->rho_p = rho_p.p; v->rho_c = rho_c.p;
+        v->rho_c_poly = kC.p + (size_t)c.M * Vn; v->rho_c_ion = kC.p + (size_t)(c.M + 1) * Vn;
+        v->ion_rho = ion_rho.p; v->drift = drift.p; v->drift_bar = drift_bar.p; v->dpsi = dpsi.p; v->dpsi_bar = dpsi_bar.p;
+    }
+};
+
+static HostCfg make_cfg(const ftsp_config* in)
+{
+    HostCfg c{};
+    c.m1 = in->m1; c.m2 = in->m2; c.m3 = in->m3;
+    if (c.m1 <= 0 || c.m2 <= 0 || c.m3 <= 0) throw std::runtime_error("invalid mesh");
+    c.V = (size_t)c.m1 * c.m2 * c.m3;
+    c.L[0] = in->L1; c.L[1] = in->L2; c.L[2] = in->L3;
+    c.volume = in->L1 * in->L2 * in->L3;
+    c.dV = in->dV; c.a = in->a; c.lB = in->lB; c.dt = in->dt; c.lpsi = in->lambda_psi;
+    c.elec = in->lB > 0.0;
+    c.M = in->M; c.nm = in->n_modes;
+    if (c.M < 1 || c.M > MAXM) throw std::runtime_error("monomer type count out of range (1..8)");
+    if (c.nm < 0 || c.nm > MAXMODE) throw std::runtime_error("active mode count out of range (0..8)");
+    for (int a = 0; a < c.nm; ++a) {
+        c.coeff.push_back(in->mode_coeff[a]);
+        c.lambda.push_back(in->mode_lambda[a]);
+        c.gamma.push_back(make_double2(in->mode_gamma[2 * a], in->mode_gamma[2 * a + 1]));
+        for (int al = 0; al < c.M; ++al) c.O.push_back(in->mode_O[a * c.M + al]);
+    }
+    if (in->n_species < 1 || in->n_species > MAXSP) throw std::runtime_error("polymer species count out of range (1..16)");
+    if (in->n_ions < 0 || in->n_ions > MAXION) throw std::runtime_error("ion species count out of range (0..16)");
+    int off = 0;
+    for (int s = 0; s < in->n_species; ++s) {
+        Species sp{};
+        sp.nc = in->num_chains[s];
+        sp.N = in->N[s];
+        if (sp.N < 1) throw std::runtime_error("species with N < 1");
+        for (int t = 0; t < sp.N; ++t) {
+            const int ty = in->seg_type[off + t];
+            if (ty < 0 || ty >= c.M) throw std::runtime_error("segment monomer type out of range");
+            sp.type.push_back(ty);
+            sp.charge.push_back(in->seg_charge[off + t]);
+            sp.bond.push_back(in->seg_bond[off + t]);
+        }
+        off += sp.N;
+        for (int t = 0; t < sp.N; ++t) {
+            const double z = c.elec ? sp.charge[t] : 0.0;
+            int k = -1;
+            for (size_t q = 0; q < c.cls.size(); ++q)
+                if (c.cls[q].type == sp.type[t] && c.cls[q].z == z) k = (int)q;
+            if (k < 0) {
+                c.cls.push_back(Cls{sp.type[t], z});
+                k = (int)c.cls.size() - 1;
+            }
+            sp.cls.push_back(k);
+        }
+        for (int t = 0; t + 1 < sp.N; ++t) {
+            int k = -1;
+            for (size_t q = 0; q < c.bond_lengths.size(); ++q)
+                if (c.bond_lengths[q] == sp.bond[t]) k = (int)q;
+            if (k < 0) {
+                c.bond_lengths.push_back(sp.bond[t]);
+                k = (int)c.bond_lengths.size() - 1;
+            }
+            sp.bcls.push_back(k);
+        }
+        c.sp.push_back(sp);
+    }
+    for (int j = 0; j < in->n_ions; ++j) c.ions.push_back(Ion{in->ion_valence[j], in->ion_count[j], in->ion_smear[j]});
+    c.self_pressure = in->self_pressure;
+    c.stress_mask = in->stress_mask & 63;
+    c.iso = in->isotropic_pressure ? 1 : 0;
+    c.noise = in->noise != 0;
+    c.seed = in->seed;
+    c.precision = in->precision;
+    c.scheme = in->scheme;
+    c.device = in->device;
+    if (c.record_len() > 128) throw std::runtime_error("observable record too long");
+    return c;
+}
+
+}  // namespace ftsp
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct ftsp_handle {
+    std::unique_ptr<ftsp::EngineBase> eng;
+    std::string err;
+};
+
+static thread_local std::string g_create_error;
+
+#define FTSP_GUARD(h, body)                                      \
+    do {                                                         \
+        if (!(h) || !(h)->eng) return FTSP_ERROR;                \
+        try {                                                    \
+            body;                                                \
+        } catch (const std::exception& e_) {                     \
+            (h)->err = e_.what();                                \
+            return FTSP_ERROR;                                   \
+        }                                                        \
+    } while (0)
+
+extern "C" {
+
+int ftsp_create(const ftsp_config* cfg, ftsp_handle** out)
+{
+    if (!cfg || !out) return FTSP_ERROR;
+    *out = nullptr;
+    try {
+        ftsp::HostCfg c = ftsp::make_cfg(cfg);
+        auto* h = new ftsp_handle();
+        if (c.precision == FTSP_FP32) h->eng.reset(new ftsp::Engine<float>(c));
+        else h->eng.reset(new ftsp::Engine<double>(c));
+        *out = h;
+        return FTSP_OK;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return FTSP_ERROR;
+    }
+}
+
+int ftsp_destroy(ftsp_handle* h)
+{
+    if (!h) return FTSP_ERROR;
+    try {
+        h->eng.reset();
+    } catch (...) {
+    }
+    delete h;
+    return FTSP_OK;
+}
+
+const char* ftsp_last_error(const ftsp_handle* h)
+{
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
+}
+
+int ftsp_set_stream(ftsp_handle* h, void* s)
+{
+    FTSP_GUARD(h, h->eng->stream = static_cast<cudaStream_t>(s));
+    return FTSP_OK;
+}
+
+int ftsp_set_fields(ftsp_handle* h, const double* omega, const double* psi)
+{
+    if (!psi) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->set_fields(omega, psi));
+    return FTSP_OK;
+}
+
+int ftsp_get_field(ftsp_handle* h, const char* name, double* out, long long* count)
+{
+    long long n = -1;
+    FTSP_GUARD(h, n = h->eng->get_field(name ? name : "", out));
+    if (count) *count = n;
+    if (n < 0) {
+        h->err = std::string("unknown field ") + (name ? name : "");
+        return FTSP_ERROR;
+    }
+    return FTSP_OK;
+}
+
+int ftsp_compute_densities(ftsp_handle* h, int which, double* Q_out)
+{
+    FTSP_GUARD(h, h->eng->compute_densities(which ? 1 : 0, Q_out));
+    for (size_t s = 0; s < h->eng->c.sp.size(); ++s)
+        if (Q_out && !(std::isfinite(Q_out[2 * s]) && std::isfinite(Q_out[2 * s + 1]))) return FTSP_NONFINITE;
+    return FTSP_OK;
+}
+
+int ftsp_record_length(const ftsp_handle* h)
+{
+    if (!h || !h->eng) return -1;
+    return h->eng->c.record_len();
+}
+
+int ftsp_measure(ftsp_handle* h, int which, double* record)
+{
+    FTSP_GUARD(h, h->eng->measure(which ? 1 : 0, record));
+    if (record)
+        for (int i = 0; i < 2 * h->eng->c.record_len(); ++i)
+            if (!std::isfinite(record[i])) return FTSP_NONFINITE;
+    return FTSP_OK;
+}
+
+int ftsp_set_noise(ftsp_handle* h, const double* eta)
+{
+    if (!eta) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->set_noise(eta));
+    return FTSP_OK;
+}
+
+int ftsp_set_seed(ftsp_handle* h, unsigned long long seed)
+{
+    FTSP_GUARD(h, h->eng->c.seed = seed);
+    return FTSP_OK;
+}
+
+int ftsp_step(ftsp_handle* h, double* Q_bar, double* record, double* drift_max)
+{
+    int st = FTSP_ERROR;
+    FTSP_GUARD(h, st = h->eng->step(Q_bar, record, drift_max, true));
+    return st;
+}
+
+int ftsp_step_async(ftsp_handle* h)
+{
+    FTSP_GUARD(h, h->eng->step(nullptr, nullptr, nullptr, false));
+    return FTSP_OK;
+}
+
+int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max)
+{
+    int st = FTSP_ERROR;
+    FTSP_GUARD(h, st = h->eng->read_status(record, drift_max));
+    return st;
+}
+
+int ftsp_state_views(ftsp_handle* h, ftsp_views* v)
+{
+    if (!v) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->views(v));
+    return FTSP_OK;
+}
+
+long long ftsp_last_launch_count(const ftsp_handle* h)
+{
+    if (!h || !h->eng) return -1;
+    return h->eng->launches;
+}
+
+}  // extern "C"

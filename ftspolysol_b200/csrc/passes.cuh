@@ -1,0 +1,369 @@
+// FFT pass kernels with fused pointwise work.
+//
+// A 3-D transform of an m1 x m2 x m3 row-major grid (z fastest) is split
+// into passes that each read and write HBM once:
+//   * plane pass   : one x-plane (m2 x m3) per CTA, z- and y-transforms in
+//                    shared memory (used when the plane fits: complex64 up
+//                    to 128^2, complex128 up to 96^2);
+//   * z-line pass  : B contiguous z-rows per CTA;
+//   * strided pass : an n x W tile of lines along y or x, W contiguous
+//                    z-columns wide, so every load and store is a W-element
+//                    contiguous run.
+// Each kernel is  [load -> transform(S1)] -> pointwise Op -> [transform(S2)
+// -> store] -> Op::end (block reductions, reusing the tile as scratch);
+// S = 0 skips that transform, -1/+1 select its sign.  The Op sees
+// the element's coordinates (in k-space after a transform) and its global
+// offset, so propagator, density, stress and smoothing work rides in the same
+// pass as the FFT instead of costing extra HBM round trips.
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace ftsp {
+
+struct PlaneGeom {
+    int m1, m2, m3;
+    int P;                 // shared-memory pitch of a plane row (m3 + 1)
+    FftPlan1 py, pz;
+};
+
+struct LineGeom {
+    int m1, m2, m3;
+    int n;                 // transform length (m1 for x, m2 for y, m3 for z)
+    int W;                 // z-columns per tile (strided passes)
+    int B;                 // rows per tile (z-line pass)
+    int P;                 // shared-memory pitch
+    FftPlan1 p;
+};
+
+// ---- block reductions (deterministic: fixed shuffle/smem order) ----
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double x = v[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[c] = x;
+    }
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) scratch[warp * K + c] = v[c];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += scratch[w * K + c];
+            v[c] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Plane pass: grid (m1, nfields), one x-plane per CTA.
+// Shared memory: tile[m2][P] + twiddles(m2) + twiddles(m3).
+// ---------------------------------------------------------------------------
+template <typename T, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(512) k_plane(PlaneGeom g, const cplx<T>* src, cplx<T>* dst,
+                                                size_t fstride, const cplx<T>* __restrict__ twy,
+                                                const cplx<T>* __restrict__ twz, Op op)
+{
+    using V = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* sty = tile + (size_t)g.m2 * g.P;
+    V* stz = sty + g.m2;
+    const int x = blockIdx.x;
+    const int f = blockIdx.y;
+    const int ne = g.m2 * g.m3;
+    const size_t base = (size_t)f * fstride + (size_t)x * ne;
+    if (S1 != 0 || S2 != 0) {
+        load_twiddles(sty, twy, g.m2);
+        load_twiddles(stz, twz, g.m3);
+    }
+    if (S1 != 0) {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int y = e / g.m3, z = e - y * g.m3;
+            tile[y * g.P + z] = src[base + e];
+        }
+        __syncthreads();
+        fft_tile<V, S1, E>(tile, stz, g.pz, g.m2, 1, g.P);
+        fft_tile<V, S1, E>(tile, sty, g.py, g.m3, g.P, 1);
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int y = e / g.m3, z = e - y * g.m3;
+        V v = S1 != 0 ? tile[y * g.P + z] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z, base + e, v);
+        if (S2 != 0) tile[y * g.P + z] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        fft_tile<V, S2, E>(tile, stz, g.pz, g.m2, 1, g.P);
+        fft_tile<V, S2, E>(tile, sty, g.py, g.m3, g.P, 1);
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int y = e / g.m3, z = e - y * g.m3;
+            dst[base + e] = tile[y * g.P + z];
+        }
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// z-line pass: grid (m1*m2/B, nfields); B rows of m3 per CTA.
+// Shared memory: tile[B][P] (P = m3 + 1) + twiddles(m3).
+// ---------------------------------------------------------------------------
+template <typename T, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(256) k_zline(LineGeom g, const cplx<T>* src, cplx<T>* dst,
+                                                size_t fstride, const cplx<T>* __restrict__ twz, Op op)
+{
+    using V = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* st = tile + (size_t)g.B * g.P;
+    const int f = blockIdx.y;
+    const int ne = g.B * g.m3;
+    const int row0 = blockIdx.x * g.B;
+    const size_t base = (size_t)f * fstride + (size_t)row0 * g.m3;
+    if (S1 != 0 || S2 != 0) load_twiddles(st, twz, g.m3);
+    if (S1 != 0) {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int b = e / g.m3, z = e - b * g.m3;
+            tile[b * g.P + z] = src[base + e];
+        }
+        __syncthreads();
+        fft_tile<V, S1, E>(tile, st, g.p, g.B, 1, g.P);
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int b = e / g.m3, z = e - b * g.m3;
+        const int row = row0 + b;
+        const int x = row / g.m2, y = row - x * g.m2;
+        V v = S1 != 0 ? tile[b * g.P + z] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z, base + e, v);
+        if (S2 != 0) tile[b * g.P + z] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        fft_tile<V, S2, E>(tile, st, g.p, g.B, 1, g.P);
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int b = e / g.m3, z = e - b * g.m3;
+            dst[base + e] = tile[b * g.P + z];
+        }
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// Strided pass along y (DIM = 1) or x (DIM = 0): grid (outer * m3/W, nf).
+// Tile[n][W] (pitch W) of lines; the outer index is x for DIM 1, y for DIM 0.
+// ---------------------------------------------------------------------------
+template <typename T, int E, int DIM, int S1, int S2, class Op>
+__global__ void __launch_bounds__(256) k_strided(LineGeom g, const cplx<T>* src, cplx<T>* dst,
+                                                  size_t fstride, const cplx<T>* __restrict__ tw, Op op)
+{
+    using V = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* st = tile + (size_t)g.n * g.W;
+    const int nzb = g.m3 / g.W;
+    const int outer = blockIdx.x / nzb;
+    const int z0 = (blockIdx.x - outer * nzb) * g.W;
+    const int f = blockIdx.y;
+    const size_t plane = (size_t)g.m2 * g.m3;
+    const size_t lstride = DIM == 1 ? (size_t)g.m3 : plane;
+    const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * g.m3) + z0;
+    const int ne = g.n * g.W;
+    if (S1 != 0 || S2 != 0) load_twiddles(st, tw, g.n);
+    if (S1 != 0) {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int j = e / g.W, w = e - j * g.W;
+            tile[e] = src[base + j * lstride + w];
+        }
+        __syncthreads();
+        fft_tile<V, S1, E>(tile, st, g.p, g.W, g.W, 1);
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int j = e / g.W, w = e - j * g.W;
+        const int x = DIM == 1 ? outer : j;
+        const int y = DIM == 1 ? j : outer;
+        const size_t off = base + j * lstride + w;
+        V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z0 + w, off, v);
+        if (S2 != 0) tile[e] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        fft_tile<V, S2, E>(tile, st, g.p, g.W, g.W, 1);
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int j = e / g.W, w = e - j * g.W;
+            dst[base + j * lstride + w] = tile[e];
+        }
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise ops
+// ---------------------------------------------------------------------------
+template <typename T>
+struct OpIdentity {
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ cplx<T> operator()(int, int, int, int, size_t, cplx<T> v) const { return v; }
+    __device__ __forceinline__ void end(double*, size_t) {}
+};
+
+// Chain-propagator pointwise work in the real-space pass of one segment.
+// KIND selects the sweep position:
+//   forward : q = u * E (u = IFFT of the previous bond, or 1 at s = 0);
+//             q is stored as qF[s]; the last segment also sums q for Q.
+//   backward: u = exp(+W_s) qB[s] (the previous transform's output, or 1 at
+//             s = N-1); phi = qF[s] * u is accumulated into the per-type
+//             and charge densities with the species factor (n/V)/Q; the
+//             propagation continues with qB[s] = u * E.
+enum PropKind { FWD_START = 0, FWD_MID = 1, FWD_LAST = 2, FWD_SINGLE = 3, BWD_START = 4, BWD_MID = 5, BWD_LAST = 6, BWD_SINGLE = 7 };
+
+template <typename T, int KIND>
+struct OpProp {
+    using V = cplx<T>;
+    const V* E;              // exp(-W) of the segment's class
+    V* qstore;               // forward: qF[s]
+    const V* qread;          // backward: qF[s]
+    V* rho_type;             // backward: density accumulator of the segment's type
+    V* rho_charge;           // backward: charge accumulator (null when z == 0)
+    T z;                     // segment valence
+    const double2* factor;   // backward: species factor (n/V)/Q
+    double2* partial;        // forward last: per-CTA sums of q
+    double acc[2];
+    T fr, fi;
+
+    __device__ __forceinline__ void begin()
+    {
+        acc[0] = acc[1] = 0.0;
+        if (KIND >= BWD_START) {
+            const double2 fc = *factor;
+            fr = T(fc.x);
+            fi = T(fc.y);
+        }
+    }
+    __device__ __forceinline__ V operator()(int, int, int, int, size_t g, V u)
+    {
+        if (KIND <= FWD_SINGLE) {
+            const V e = E[g];
+            const V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? e : cmul(u, e);
+            qstore[g] = q;
+            if (KIND == FWD_LAST || KIND == FWD_SINGLE) {
+                acc[0] += (double)q.x;
+                acc[1] += (double)q.y;
+            }
+            return q;
+        } else {
+            const V qf = qread[g];
+            const V phi = (KIND == BWD_START || KIND == BWD_SINGLE) ? qf : cmul(qf, u);
+            const V w = cmul(phi, mkc<V>(fr, fi));
+            V r = rho_type[g];
+            rho_type[g] = cadd(r, w);
+            if (rho_charge) {
+                V c = rho_charge[g];
+                rho_charge[g] = cadd(c, cscale(w, z));
+            }
+            if (KIND == BWD_START) return E[g];
+            if (KIND == BWD_MID) return cmul(u, E[g]);
+            return u;
+        }
+    }
+    __device__ __forceinline__ void end(double* scratch, size_t cta)
+    {
+        if (KIND == FWD_LAST || KIND == FWD_SINGLE) {
+            __syncthreads();
+            block_sum<2>(acc, scratch);
+            if (threadIdx.x == 0) partial[cta] = make_double2(acc[0], acc[1]);
+        }
+    }
+};
+
+// Bond pointwise work in the k-space (x) pass of one bond s -> s+1.
+//   forward : F = DFT(qF[s]) (sign -1); optionally stored for the stress;
+//             output F * Phi_s / V.
+//   backward: B' = DFT_{+}(qB[s+1]) (sign +1, i.e. B(-k)); optionally the
+//             connectivity stress sums  sum_k k_a k_b Phi_s F_s B'  (weighted
+//             by b_s^2 and the species factor) are accumulated; output
+//             B' * Phi_s / V.
+// Phi_s(k) = exp(-b^2 k^2/6) is separable: phix[kx] phiy[ky] phiz[kz].
+template <typename T, bool FWD, bool STRESS>
+struct OpBond {
+    using V = cplx<T>;
+    V* Fstore;
+    const V* Fread;
+    const T* phix;
+    const T* phiy;
+    const T* phiz;
+    const double* kx;
+    const double* ky;
+    const double* kz;
+    T invV;
+    double b2;
+    const double2* factor;
+    double2* partial;        // [cta][6] accumulated across bonds
+    double acc[12];
+
+    __device__ __forceinline__ void begin()
+    {
+        if (STRESS) {
+#pragma unroll
+            for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+        }
+    }
+    __device__ __forceinline__ V operator()(int, int x, int y, int z, size_t g, V v)
+    {
+        const T phi = phix[x] * phiy[y] * phiz[z];
+        if (FWD) {
+            if (Fstore) Fstore[g] = v;
+        } else if (STRESS) {
+            const V F = Fread[g];
+            const V p = cmul(F, v);
+            const double pr = (double)p.x * (double)phi, pi = (double)p.y * (double)phi;
+            const double ax = kx[x], ay = ky[y], az = kz[z];
+            const double kk[6] = {ax * ax, ay * ay, az * az, ax * ay, ax * az, ay * az};
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                acc[2 * c] += kk[c] * pr;
+                acc[2 * c + 1] += kk[c] * pi;
+            }
+        }
+        return cscale(v, phi * invV);
+    }
+    __device__ __forceinline__ void end(double* scratch, size_t cta)
+    {
+        if (STRESS) {
+            __syncthreads();
+            block_sum<12>(acc, scratch);
+            if (threadIdx.x == 0) {
+                const double2 fc = *factor;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    const double sr = b2 * acc[2 * c], si = b2 * acc[2 * c + 1];
+                    double2 o = partial[cta * 6 + c];
+                    o.x += sr * fc.x - si * fc.y;
+                    o.y += sr * fc.y + si * fc.x;
+                    partial[cta * 6 + c] = o;
+                }
+            }
+        }
+    }
+};
+
+}  // namespace ftsp

@@ -1,0 +1,277 @@
+"""Python front end of libftsp.so (the engine's C ABI, include/ftsp.h).
+
+Mirrors the reference's step-loop surface: compute_densities
+(complexLangevin.cu:255-260), measure (observable.cu:53-67), step
+(complexLangevin.cu:669-698), the deviceState field names
+(deviceState.h:6-48).  The CUDA library is the only implementation: if it
+cannot be loaded, or no CUDA device is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libftsp.so")
+
+FTSP_OK, FTSP_NONFINITE, FTSP_ERROR, FTSP_TIMEOUT = 0, 1, 2, 3
+FP64, FP32 = 0, 1
+SCHEME_PC, SCHEME_SI = 0, 1
+STRESS_NAMES = ("xx", "yy", "zz", "xy", "xz", "yz")
+
+
+class FtspError(RuntimeError):
+    pass
+
+
+class NonFinite(RuntimeError):
+    pass
+
+
+class ftsp_config(C.Structure):
+    _fields_ = [
+        ("m1", C.c_int), ("m2", C.c_int), ("m3", C.c_int),
+        ("L1", C.c_double), ("L2", C.c_double), ("L3", C.c_double),
+        ("dV", C.c_double), ("a", C.c_double), ("lB", C.c_double), ("dt", C.c_double),
+        ("lambda_psi", C.c_double),
+        ("M", C.c_int), ("n_modes", C.c_int),
+        ("mode_coeff", C.POINTER(C.c_double)), ("mode_gamma", C.POINTER(C.c_double)),
+        ("mode_O", C.POINTER(C.c_double)), ("mode_lambda", C.POINTER(C.c_double)),
+        ("n_species", C.c_int), ("num_chains", C.POINTER(C.c_double)), ("N", C.POINTER(C.c_int)),
+        ("seg_type", C.POINTER(C.c_int)), ("seg_charge", C.POINTER(C.c_double)),
+        ("seg_bond", C.POINTER(C.c_double)),
+        ("n_ions", C.c_int), ("ion_valence", C.POINTER(C.c_double)), ("ion_count", C.POINTER(C.c_double)),
+        ("ion_smear", C.POINTER(C.c_double)),
+        ("self_pressure", C.c_double), ("stress_mask", C.c_int), ("isotropic_pressure", C.c_int),
+        ("noise", C.c_int), ("seed", C.c_ulonglong), ("precision", C.c_int), ("scheme", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class ftsp_views(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("omega", "psi", "omega_bar", "psi_bar", "rho_type", "rho_p", "rho_c",
+                                          "rho_c_poly", "rho_c_ion", "ion_rho", "drift", "drift_bar", "dpsi",
+                                          "dpsi_bar")]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib():
+    """Loads libftsp.so (building it first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _b
+            _b.build()
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.ftsp_create.argtypes = [C.POINTER(ftsp_config), C.POINTER(vp)]
+        L.ftsp_destroy.argtypes = [vp]
+        L.ftsp_last_error.restype = C.c_char_p
+        L.ftsp_last_error.argtypes = [vp]
+        L.ftsp_set_stream.argtypes = [vp, vp]
+        L.ftsp_set_fields.argtypes = [vp, vp, vp]
+        L.ftsp_get_field.argtypes = [vp, C.c_char_p, vp, C.POINTER(C.c_longlong)]
+        L.ftsp_compute_densities.argtypes = [vp, C.c_int, vp]
+        L.ftsp_record_length.argtypes = [vp]
+        L.ftsp_measure.argtypes = [vp, C.c_int, vp]
+        L.ftsp_set_noise.argtypes = [vp, vp]
+        L.ftsp_set_seed.argtypes = [vp, C.c_ulonglong]
+        L.ftsp_step.argtypes = [vp, vp, vp, vp]
+        L.ftsp_step_async.argtypes = [vp]
+        L.ftsp_read_status.argtypes = [vp, vp, vp]
+        L.ftsp_state_views.argtypes = [vp, C.POINTER(ftsp_views)]
+        L.ftsp_last_launch_count.restype = C.c_longlong
+        L.ftsp_last_launch_count.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+# exported symbols of include/ftsp.h
+ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_stream", "ftsp_set_fields",
+               "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
+               "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
+               "ftsp_state_views", "ftsp_last_launch_count")
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Engine:
+    """One complex-Langevin system on one GPU.
+
+    `derived` holds the derived parameters (the output of the host-side
+    param/sequence/ion setup): m, L, dV, a, lB, dt, lambda_psi, M, modes
+    [{coeff, lambda, gamma, O}], species [{num_chains, types, charges,
+    bonds}], ions [{valence, count, smear}], self_pressure, stress (component
+    names), isotropic_pressure.
+    """
+
+    def __init__(self, derived: dict, precision: int = FP64, scheme: int = SCHEME_PC, noise: bool = False,
+                 seed: int = 0, device: int = 0):
+        L = lib()
+        self._keep = []
+
+        def arr(x, dt=np.float64):
+            a = np.ascontiguousarray(np.asarray(x, dtype=dt))
+            if a.size == 0:
+                a = np.zeros(1, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        d = derived
+        self.m = tuple(int(v) for v in d["m"])
+        self.size = int(np.prod(self.m))
+        modes = d["modes"]
+        self.n_modes = len(modes)
+        self.M = int(d["M"])
+        sp = d["species"]
+        self.n_species = len(sp)
+        self.n_ions = len(d["ions"])
+        cfg = ftsp_config()
+        cfg.m1, cfg.m2, cfg.m3 = self.m
+        cfg.L1, cfg.L2, cfg.L3 = [float(v) for v in d["L"]]
+        cfg.dV = float(d["dV"])
+        cfg.a = float(d["a"])
+        cfg.lB = float(d["lB"])
+        cfg.dt = float(d["dt"])
+        cfg.lambda_psi = float(d["lambda_psi"])
+        cfg.M = self.M
+        cfg.n_modes = self.n_modes
+        cfg.mode_coeff = _dp(arr([m["coeff"] for m in modes]))
+        g = []
+        for m in modes:
+            g += [complex(m["gamma"]).real, complex(m["gamma"]).imag]
+        cfg.mode_gamma = _dp(arr(g))
+        cfg.mode_O = _dp(arr([o for m in modes for o in m["O"]]))
+        cfg.mode_lambda = _dp(arr([m["lambda"] for m in modes]))
+        cfg.n_species = len(sp)
+        cfg.num_chains = _dp(arr([s["num_chains"] for s in sp]))
+        cfg.N = _ip(arr([len(s["types"]) for s in sp], np.int32))
+        cfg.seg_type = _ip(arr([t for s in sp for t in s["types"]], np.int32))
+        cfg.seg_charge = _dp(arr([q for s in sp for q in s["charges"]]))
+        cfg.seg_bond = _dp(arr([b for s in sp for b in s["bonds"]]))
+        ions = d["ions"]
+        cfg.n_ions = len(ions)
+        cfg.ion_valence = _dp(arr([i["valence"] for i in ions]))
+        cfg.ion_count = _dp(arr([i["count"] for i in ions]))
+        cfg.ion_smear = _dp(arr([i["smear"] for i in ions]))
+        cfg.self_pressure = float(d["self_pressure"])
+        mask = 0
+        for c in d.get("stress", ()):
+            mask |= 1 << STRESS_NAMES.index(c)
+        cfg.stress_mask = mask
+        cfg.isotropic_pressure = int(bool(d.get("isotropic_pressure", False)))
+        cfg.noise = int(bool(noise))
+        cfg.seed = int(seed)
+        cfg.precision = int(precision)
+        cfg.scheme = int(scheme)
+        cfg.device = int(device)
+        self.precision = precision
+        self._cfg = cfg
+        h = C.c_void_p()
+        rc = L.ftsp_create(C.byref(cfg), C.byref(h))
+        if rc != FTSP_OK:
+            raise FtspError("ftsp_create failed: " + (L.ftsp_last_error(None) or b"").decode())
+        self.h = h
+        self.record_len = L.ftsp_record_length(self.h)
+
+    # ---- helpers ----
+    def _check(self, rc, what):
+        if rc == FTSP_OK:
+            return rc
+        if rc == FTSP_NONFINITE:
+            raise NonFinite(what + ": non-finite value")
+        raise FtspError(what + ": " + (lib().ftsp_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ftsp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- API ----
+    def set_fields(self, omega, psi):
+        o = np.ascontiguousarray(np.asarray(omega, dtype=np.complex128).reshape(self.n_modes, self.size))
+        p = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128).reshape(self.size))
+        if o.size == 0:
+            o = np.zeros(1, dtype=np.complex128)
+        self._check(lib().ftsp_set_fields(self.h, o.ctypes.data, p.ctypes.data), "set_fields")
+
+    def get(self, name: str) -> np.ndarray:
+        n = C.c_longlong(0)
+        self._check(lib().ftsp_get_field(self.h, name.encode(), None, C.byref(n)), "get_field")
+        out = np.zeros(max(1, n.value), dtype=np.float64)
+        self._check(lib().ftsp_get_field(self.h, name.encode(), out.ctypes.data, C.byref(n)), "get_field")
+        return out[: n.value].view(np.complex128).reshape(-1, self.size)
+
+    def compute_densities(self, which: int = 0) -> np.ndarray:
+        Q = np.zeros(max(1, self.n_species), dtype=np.complex128)
+        self._check(lib().ftsp_compute_densities(self.h, which, Q.ctypes.data), "compute_densities")
+        return Q[: self.n_species]
+
+    def measure(self, which: int = 0) -> np.ndarray:
+        rec = np.zeros(self.record_len, dtype=np.complex128)
+        self._check(lib().ftsp_measure(self.h, which, rec.ctypes.data), "measure")
+        return rec
+
+    def set_noise(self, eta):
+        e = np.ascontiguousarray(np.asarray(eta, dtype=np.float64).reshape(-1))
+        if e.size != (self.n_modes + 1) * self.size:
+            raise ValueError("noise must hold (n_modes + 1) * V values")
+        self._check(lib().ftsp_set_noise(self.h, e.ctypes.data), "set_noise")
+
+    def step(self, eta=None):
+        """One step; returns (Q_bar, record, drift_max)."""
+        if eta is not None:
+            self.set_noise(eta)
+        Qb = np.zeros(max(1, self.n_species), dtype=np.complex128)
+        rec = np.zeros(max(1, self.record_len), dtype=np.complex128)
+        dmax = np.zeros(self.n_modes + 1)
+        self._check(lib().ftsp_step(self.h, Qb.ctypes.data, rec.ctypes.data, dmax.ctypes.data), "step")
+        return Qb[: self.n_species], rec[: self.record_len], dmax
+
+    def step_async(self):
+        self._check(lib().ftsp_step_async(self.h), "step_async")
+
+    def read_status(self):
+        rec = np.zeros(max(1, self.record_len), dtype=np.complex128)
+        dmax = np.zeros(self.n_modes + 1)
+        rc = lib().ftsp_read_status(self.h, rec.ctypes.data, dmax.ctypes.data)
+        return rc, rec[: self.record_len], dmax
+
+    def set_stream(self, stream_handle: int):
+        self._check(lib().ftsp_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def launches(self) -> int:
+        return int(lib().ftsp_last_launch_count(self.h))
+
+    def views(self) -> ftsp_views:
+        v = ftsp_views()
+        self._check(lib().ftsp_state_views(self.h, C.byref(v)), "state_views")
+        return v
