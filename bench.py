@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark: complex-Langevin steps/s on the 128^3, N = 50 polyelectrolyte
+workload (L = 64 b, bead density 0.5 b^-3, v = 0.1 b^3, lB = 1 b, divalent
+counterions, 1:1 salt at 0.05 b^-3, full stress tensor and isotropic
+pressure every step, seeded Langevin noise, complex64 propagators and fields
+with FP64 reductions).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full predictor-corrector CL step (two density evaluations,
+both chain-propagator sweeps, observables, update).  Under torchrun each rank
+runs its own independent replica (different seed): weak scaling, no
+collective in the data path; the elapsed time is the max over ranks.
+
+Prints one JSON line.  `--impl reference` times the reference's own CUDA
+build (oracle/_ref/ref_harness, built from the reference sources by
+oracle/build_ref.sh) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CL steps/s at 128^3 N=50"
+UNIT = "steps/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--grid", type=int, default=128, help="override the grid (small smoke runs only)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-line", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the propagator passes from the committed ncu
+    summary (profiles/propagator_passes_128cube_N50.md, lines 'traffic <kind> <bytes>')."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "propagator_passes_128cube_N50.md")
+    if os.path.exists(path):
+        for line in open(path):
+            p = line.split()
+            if len(p) == 3 and p[0] == "traffic":
+                try:
+                    out[p[1]] = float(p[2])
+                except ValueError:
+                    pass
+    return out
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle on the host cores
+# ---------------------------------------------------------------------------
+def cpu_baseline(case, derived):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    po.build()
+    threads = po.lib().oracle_threads()
+    # cost ratio full step / one density evaluation, measured on a small grid
+    # of the same chemistry
+    from ftspolysol_b200.cases import workload
+    from ftspolysol_b200.derive import derive
+    small = workload(4, noise=False)
+    small.m = (32, 32, 32)
+    small.salt = dict(small.salt)
+    V = (32 * small.dL) ** 3
+    small.species[0].num_chains = int(round(0.5 * V / 50))
+    small.salt["num_salt"] = int(round(0.05 * V))
+    ds = derive(small)
+    o = po.Oracle(ds)
+    om, ps = small.initial_fields()
+    o.set_fields(om, ps)
+    t0 = time.perf_counter()
+    o.compute_densities(0)
+    t1 = time.perf_counter()
+    o.step(None)
+    t2 = time.perf_counter()
+    ratio = (t2 - t1) / (t1 - t0)
+    o.close()
+    # the workload itself: one density evaluation at full size
+    o = po.Oracle(derived)
+    om, ps = case.initial_fields()
+    o.set_fields(om, ps)
+    t0 = time.perf_counter()
+    o.compute_densities(0)
+    t_dens = time.perf_counter() - t0
+    o.close()
+    step_s = t_dens * ratio
+    return {"value": 1.0 / step_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": ("one FP64 density evaluation of the 128^3 N=50 workload (%.1f s) times the measured "
+                       "full-step/density-evaluation cost ratio of the oracle (%.2f, on 32^3 N=50 of the same "
+                       "chemistry); the oracle restates the reference's step including its stress re-solves"
+                       % (t_dens, ratio))}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference"}
+    if not os.path.exists(harness):
+        ref_src = "/root/reference"
+        if os.path.isdir(ref_src):
+            subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh"), ref_src], check=False,
+                           stdout=subprocess.DEVNULL)
+    if not os.path.exists(harness):
+        base["unavailable"] = "reference CUDA build (oracle/_ref/ref_harness) is missing and cannot be built here"
+        print(json.dumps(base))
+        return 0
+    from ftspolysol_b200.cases import workload
+    case = workload(4, noise=True)
+    if args.grid != 128:
+        case = scaled_case(case, args.grid)
+    work = tempfile.mkdtemp(prefix="ftsp_ref_")
+    paths = case.write(work)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    res = subprocess.run([harness, "time", os.path.basename(paths["param"]), paths["omega"], paths["psi"],
+                          str(args.warmup), str(args.steps)], cwd=work, capture_output=True, text=True)
+    ck = clocks.stop()
+    if res.returncode != 0:
+        base["unavailable"] = "reference CUDA build failed on this workload: " + res.stderr.strip()[-200:]
+        print(json.dumps(base))
+        return 0
+    r = json.loads(res.stdout.strip().splitlines()[-1])
+    value = r["steps_per_s"]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["event_ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": case.name + ": 128^3 grid, L=64b, N=50, divalent counterions, 1:1 salt 0.05, "
+                                                "full stress + isotropic pressure every step, seeded noise",
+                       "scheme": "predictor-corrector (reference)", "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": "the reference's own CUDA build (FP64, cuFFT) on the same B200, %d timed steps"
+                                       " after %d warm-up steps; one host thread drives it" % (args.steps, args.warmup)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": ck}
+    print(json.dumps(line))
+    return 0
+
+
+def scaled_case(case, m):
+    """The same chemistry on an m^3 grid (dL unchanged)."""
+    c = case
+    V = (m * c.dL) ** 3
+    c.m = (m, m, m)
+    c.species[0].num_chains = int(round(0.5 * V / c.species[0].N))
+    if c.salt is not None:
+        c.salt = dict(c.salt)
+        c.salt["num_salt"] = int(round(0.05 * V))
+    return c
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+    from ftspolysol_b200 import Engine, FP32, FP64
+    from ftspolysol_b200.cases import workload
+    from ftspolysol_b200.derive import derive
+
+    torch.cuda.set_device(local)
+    case = workload(4, noise=True)
+    if args.grid != 128:
+        case = scaled_case(case, args.grid)
+    derived = derive(case)
+    prec = FP32 if args.precision == "fp32" else FP64
+    eng = Engine(derived, precision=prec, noise=True, seed=1234 + rank, device=local)
+    om, ps = case.initial_fields()
+    eng.set_fields(om, ps)
+    for _ in range(args.warmup):
+        eng.step_async()
+    torch.cuda.synchronize()
+    st, _, _ = eng.read_status()
+    if st != 0:
+        raise RuntimeError("warm-up steps did not finish with finite fields (status %d)" % st)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    eng.profile(True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        eng.step_async()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches_per_step = eng.launches()
+    prof = eng.profile_read()
+    eng.profile(False)
+    status, rec, _ = eng.read_status()
+    if status != 0:
+        raise RuntimeError("timed steps produced a non-finite status (%d)" % status)
+    ms_max = dist_max(ms, ws)
+    value = ws * args.steps / (ms_max * 1e-3)
+
+    # roofline of the dominant propagator pass (largest total device time)
+    peak, peak_kind = measured_peak_hbm()
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    dname, dstat = dom
+    per_launch_ms = dstat["ms"] / dstat["launches"]
+    per_launch_bytes = dstat["bytes"] / dstat["launches"]
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = committed_traffic().get(dname)
+    prop_ms = sum(v["ms"] for v in prof.values())
+    prop_bytes = sum(v["bytes"] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "traffic": traffic, "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
+                "all_propagator_passes": {"achieved": prop_bytes / (prop_ms * 1e-3) / 1e9,
+                                          "share_of_step": prop_ms / ms,
+                                          "per_kind": {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / v["launches"],
+                                                           "GBps": v["bytes"] / v["ms"] * 1e-6}
+                                                       for k, v in sorted(prof.items())}}}
+
+    # end to end through the public API: host fields in, record out, every step
+    e2e = None
+    if not args.no_e2e:
+        n_in = (eng.n_modes + 1) * eng.size
+        host = torch.empty(2 * n_in, dtype=torch.float64, pin_memory=True)
+        fields = np.concatenate([np.asarray(om).reshape(-1), np.asarray(ps).reshape(-1)])
+        host.numpy()[:] = fields.view(np.float64)
+        p_om = host.data_ptr()
+        p_ps = host.data_ptr() + eng.n_modes * eng.size * 16
+        ke = max(3, min(args.steps, 10))
+        eng.set_fields_ptr(p_om, p_ps)
+        eng.step()
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            eng.set_fields_ptr(p_om, p_ps)
+            eng.step()
+        t1 = time.perf_counter()
+        barrier(ws)
+        e_s = dist_max(t1 - t0, ws)
+        e2e = {"value": ws * ke / e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * n_in,
+               "d2h_bytes_per_step": 16 * (eng.record_len + eng.n_species) + 8 * (eng.n_modes + 1),
+               "steps": ke, "api": "ftsp_set_fields + ftsp_step (host pinned fields in, record out)"}
+    eng.close()
+
+    extra = {}
+    if rank == 0 and ws == 1 and not args.no_fp64_line and prec == FP32:
+        e64 = Engine(derived, precision=FP64, noise=True, seed=99, device=local)
+        e64.set_fields(om, ps)
+        for _ in range(2):
+            e64.step_async()
+        torch.cuda.synchronize()
+        k64 = max(3, args.steps // 4)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(k64):
+            e64.step_async()
+        a1.record()
+        torch.cuda.synchronize()
+        st64, _, _ = e64.read_status()
+        ms64 = a0.elapsed_time(a1)
+        extra["fp64"] = {"steps_per_s": k64 / (ms64 * 1e-3), "ms_per_step": ms64 / k64, "steps": k64,
+                         "status": int(st64), "dtype": "c128"}
+        e64.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case, derived)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64" if prec == FP32 else "c128",
+                "data": "synthetic",
+                "config": {"workload": case.name + ": %d^3 grid, L=%gb, N=50, divalent counterions, 1:1 salt 0.05, "
+                                                   "full stress + isotropic pressure every step, seeded noise"
+                                       % (case.m[0], case.L[0]),
+                           "precision": ("complex64 fields and propagators, FP64 reductions" if prec == FP32
+                                         else "complex128 throughout"),
+                           "scheme": "predictor-corrector", "replicas_per_gpu": 1,
+                           "parallelism": "replicas (one independent system per GPU)",
+                           "l2": "inputs larger than L2 (propagator storage %.2f GB per solve)"
+                                 % (2 * 50 * derived_bytes(case, prec) / 1e9)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+                "clocks": ck}
+        line.update(extra)
+        print(json.dumps(line))
+    return 0
+
+
+def derived_bytes(case, prec):
+    import numpy as np
+    return int(np.prod(case.m)) * (8 if prec == 1 else 16)
+
+
+def main():
+    args = parse_args()
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, ws, rank)
+        else:
+            rc = run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -19,8 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libftsp.so")
 
-SOURCES = ["engine.cu"]
-HEADERS = ["fft_core.cuh", "passes.cuh"]
+SOURCES = ["engine_f32.cu", "engine_f64.cu", "abi.cu"]
+HEADERS = ["fft_core.cuh", "passes.cuh", "engine.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-O2",
          "-Xptxas", "-warn-spills"]
@@ -40,20 +40,37 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compiles each translation unit in parallel, then links libftsp.so."""
     if not force and not _stale():
         return LIB
-    cmd = [nvcc()] + ARCH + FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    if extra:
-        cmd += list(extra)
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [nvcc()] + ARCH + FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        if extra:
+            cmd += list(extra)
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = []
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append(src)
+            sys.stderr.write(out)
+        elif verbose and out:
+            print(out)
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
+    link = [nvcc()] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libftsp.so")
-    if verbose and (res.stdout or res.stderr):
-        print(res.stdout + res.stderr)
+        raise RuntimeError("linking libftsp.so failed")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,10 +1,13 @@
 // B200 complex-Langevin engine: device state, FFT executor, chain
-// propagators, densities, Langevin update and observables.
+// propagators, densities, Langevin update and observables.  Included by
+// engine_f32.cu and engine_f64.cu (one instantiation each, compiled in
+// parallel) and by abi.cu (the C ABI; no instantiation).
 //
 // One Engine<T> per system; T = double (FP64, reference-equivalent) or
 // float (complex64 fields and propagators, FP64 reductions).  All device
 // work of a handle is queued on one stream; a step needs no host
 // synchronisation except the final status read in ftsp_step.
+#pragma once
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -107,19 +110,36 @@ struct HostCfg {
     }
 };
 
+// Radix plan: the power-of-two part in as few stages of radix <= 16 as
+// possible, spread evenly (128 = 16 x 8, 64 = 8 x 8, 32 = 8 x 4), then the
+// factors 3 and 5.
 static FftPlan1 make_plan(int n)
 {
     FftPlan1 p{};
     p.n = n;
     p.nst = 0;
-    int r = n;
-    while (r % 8 == 0 && r > 8) { p.rad[p.nst++] = 8; r /= 8; }
-    if (r == 8) { p.rad[p.nst++] = 8; r = 1; }
-    while (r % 4 == 0) { p.rad[p.nst++] = 4; r /= 4; }
-    while (r % 2 == 0) { p.rad[p.nst++] = 2; r /= 2; }
-    while (r % 3 == 0) { p.rad[p.nst++] = 3; r /= 3; }
-    while (r % 5 == 0) { p.rad[p.nst++] = 5; r /= 5; }
-    if (r != 1 || p.nst > 12) throw std::runtime_error("grid size " + std::to_string(n) + " is not 2/3/5-smooth");
+    int r = n, p2 = 0;
+    while (r % 2 == 0) {
+        r /= 2;
+        ++p2;
+    }
+    const int nst2 = (p2 + 3) / 4;
+    int left = p2;
+    for (int st = 0; st < nst2; ++st) {
+        const int bits = (left + (nst2 - st) - 1) / (nst2 - st);   // ceil(bits left / stages left)
+        p.rad[p.nst++] = 1 << bits;
+        left -= bits;
+    }
+    while (r % 3 == 0 && p.nst < 8) { p.rad[p.nst++] = 3; r /= 3; }
+    while (r % 5 == 0 && p.nst < 8) { p.rad[p.nst++] = 5; r /= 5; }
+    if (r != 1) throw std::runtime_error("grid size " + std::to_string(n) + " is not 2/3/5-smooth or needs more than 8 stages");
+    int span = 1;
+    for (int st = 0; st < p.nst; ++st) {
+        p.span[st] = span;
+        p.fspan[st] = make_fastdiv((unsigned)span);
+        p.tstep[st] = n / (p.rad[st] * span);
+        span *= p.rad[st];
+    }
     return p;
 }
 
@@ -312,11 +332,91 @@ struct OpLoadOne {
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
+struct ProfStat {
+    double ms = 0.0;
+    long long launches = 0;
+    double bytes = 0.0;   // algorithmic bytes (minimum HBM traffic of the launch's work)
+};
+
 struct EngineBase {
     HostCfg c;
     std::string err;
     cudaStream_t stream = nullptr;
     long long launches = 0;
+    // per-kernel CUDA-event timing of the propagator passes (ftsp_profile_*)
+    bool profiling = false;
+    std::vector<std::pair<std::string, ProfStat>> prof;
+    struct Pending {
+        int slot;
+        double bytes;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+
+    int prof_slot(const std::string& name)
+    {
+        for (size_t i = 0; i < prof.size(); ++i)
+            if (prof[i].first == name) return (int)i;
+        prof.push_back({name, ProfStat{}});
+        return (int)prof.size() - 1;
+    }
+    cudaEvent_t take_event()
+    {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            FTSP_CUDA(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t prof_begin()
+    {
+        if (!profiling) return nullptr;
+        cudaEvent_t a = take_event();
+        FTSP_CUDA(cudaEventRecord(a, stream));
+        return a;
+    }
+    void prof_end(cudaEvent_t a, const std::string& name, double bytes)
+    {
+        if (!profiling || !a) return;
+        cudaEvent_t b = take_event();
+        FTSP_CUDA(cudaEventRecord(b, stream));
+        pending.push_back(Pending{prof_slot(name), bytes, a, b});
+    }
+    void prof_collect()
+    {
+        if (pending.empty()) return;
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        for (auto& p : pending) {
+            float ms = 0.0f;
+            FTSP_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+            ProfStat& s = prof[p.slot].second;
+            s.ms += ms;
+            s.launches += 1;
+            s.bytes += p.bytes;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void prof_reset()
+    {
+        prof_collect();
+        prof.clear();
+    }
+    virtual void release_events()
+    {
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        pending.clear();
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
     virtual ~EngineBase() {}
     virtual void set_fields(const double* omega, const double* psi) = 0;
     virtual long long get_field(const std::string& name, double* out) = 0;
@@ -353,8 +453,12 @@ struct Engine : EngineBase {
     LineGeom gx{}, gy{}, gz{};
     int plane_threads = 0, x_threads = 0, y_threads = 0, z_threads = 0;
     size_t plane_smem = 0, x_smem = 0, y_smem = 0, z_smem = 0;
-    static constexpr int EP = sizeof(T) == 4 ? 32 : 16;   // elements per thread, plane pass
-    static constexpr int EL = 16;                          // elements per thread, line passes
+    static constexpr bool F32 = sizeof(T) == 4;
+    static constexpr int EP = F32 ? 32 : 16;   // elements per thread, runtime-plan plane pass
+    static constexpr int EL = F32 ? 16 : 8;    // elements per thread, runtime-plan line passes
+    static constexpr int RMAX = F32 ? 16 : 8;  // largest radix of the compile-time transforms
+    static constexpr int WCT = F32 ? 32 : 16;  // z-columns per tile of the compile-time strided passes
+    Buf<FftPlan1> plans;                       // device-memory plans: x, y, z
 
     // device buffers
     Buf<V> tw1, tw2, tw3;
@@ -394,9 +498,11 @@ struct Engine : EngineBase {
         Buf<V>* vb[] = {&tw1, &tw2, &tw3, &omega, &psi, &omega_bar, &psi_bar, &drift, &drift_bar, &dpsi, &dpsi_bar,
                         &kA, &kB, &dB, &kC, &rho_p, &rho_c, &ion_rho, &E, &qF, &Fst, &G, &H};
         for (auto* b : vb) b->release();
+        plans.release();
         kx.release(); ky.release(); kz.release(); phi.release(); gam.release(); gion.release(); eta.release();
-        part.release(); spart.release();
+        part.release(); spart.release(); stage.release();
         if (ds) cudaFree(ds);
+        release_events();
     }
 
     // ---- geometry and launch shapes ----
@@ -422,16 +528,21 @@ struct Engine : EngineBase {
         int dev_smem = 0;
         FTSP_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
         pg.m1 = m1; pg.m2 = m2; pg.m3 = m3; pg.P = m3 + 1;
-        pg.py = make_plan(m2);
-        pg.pz = make_plan(m3);
+        const FftPlan1 hp[3] = {make_plan(m1), make_plan(m2), make_plan(m3)};
+        plans.alloc(3);
+        FTSP_CUDA(cudaMemcpy(plans.p, hp, sizeof(hp), cudaMemcpyHostToDevice));
+        pg.py = plans.p + 1;
+        pg.pz = plans.p + 2;
+        pg.fm2 = make_fastdiv(m2);
+        pg.fm3 = make_fastdiv(m3);
         plane_smem = sizeof(V) * ((size_t)m2 * pg.P + m2 + m3);
         plane_smem = std::max(plane_smem, (size_t)32 * 16 * 8);
         plane_threads = round32((m2 * m3 + EP - 1) / EP);
         plane_ok = plane_smem <= (size_t)dev_smem && plane_threads <= 512;
         const int wmax = std::max(1, std::min(sizeof(T) == 4 ? 32 : 16, (EL * 256) / std::max(m1, m2)));
         const int W = pick_W(m3, wmax);
-        gx = LineGeom{m1, m2, m3, m1, W, 0, W, make_plan(m1)};
-        gy = LineGeom{m1, m2, m3, m2, W, 0, W, make_plan(m2)};
+        gx = LineGeom{m1, m2, m3, m1, W, 0, W, plans.p + 0, make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
+        gy = LineGeom{m1, m2, m3, m2, W, 0, W, plans.p + 1, make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
         x_threads = round32((m1 * W + EL - 1) / EL);
         y_threads = round32((m2 * W + EL - 1) / EL);
         x_smem = std::max(sizeof(V) * ((size_t)m1 * W + m1), (size_t)32 * 16 * 8);
@@ -440,7 +551,7 @@ struct Engine : EngineBase {
         if (m3 > EL * 256) throw std::runtime_error("z extent too large for the line passes");
         int B = std::max(1, 2048 / m3);
         while ((m1 * m2) % B) --B;
-        gz = LineGeom{m1, m2, m3, m3, 0, B, m3 + 1, make_plan(m3)};
+        gz = LineGeom{m1, m2, m3, m3, 0, B, m3 + 1, plans.p + 2, make_fastdiv(1), make_fastdiv(B), make_fastdiv(m2), make_fastdiv(m3)};
         z_threads = round32((B * m3 + EL - 1) / EL);
         z_smem = std::max(sizeof(V) * ((size_t)B * (m3 + 1) + m3), (size_t)32 * 16 * 8);
         if (x_threads > 256 || y_threads > 256 || z_threads > 256) throw std::runtime_error("grid dimension too large for the line passes");
@@ -551,77 +662,178 @@ struct Engine : EngineBase {
 
     // Batched in-place (or out-of-place from per-field sources) 3-D FFT of nf
     // contiguous fields of dst.  src[f] (optional) gives the input of field f.
+    // ---- pass launchers: compile-time kernels for the production lengths
+    // (32, 64, 128), runtime-plan kernels for every other 2/3/5-smooth grid ----
+    template <int N> static constexpr bool plane_ct_ok() { return F32 ? (N == 32 || N == 64 || N == 128) : (N == 32 || N == 64); }
+
+    template <int N, int S1, int S2, class Op>
+    void plane_ct(const V* src, V* dst, int nf, const Op& op)
+    {
+        constexpr int E = F32 ? (N >= 128 ? 32 : 16) : (N >= 64 ? 16 : 8);
+        constexpr int NT = N * N / E;
+        auto k = k_plane_ct<T, N, RMAX, NT, E, S1, S2, Op>;
+        const size_t smem = std::max(sizeof(V) * (size_t)(N * (N + 1) + N), (size_t)4096);
+        set_smem(k, smem);
+        k<<<dim3(c.m1, nf), NT, smem, stream>>>(src, dst, V_, tw3.p, op);
+        ++launches;
+    }
+
+    template <int S1, int S2, class Op>
+    void plane(const V* src, V* dst, int nf, const Op& op)
+    {
+        if (c.m2 == c.m3) {
+            if constexpr (plane_ct_ok<128>())
+                if (c.m3 == 128) return plane_ct<128, S1, S2>(src, dst, nf, op);
+            if constexpr (plane_ct_ok<64>())
+                if (c.m3 == 64) return plane_ct<64, S1, S2>(src, dst, nf, op);
+            if constexpr (plane_ct_ok<32>())
+                if (c.m3 == 32) return plane_ct<32, S1, S2>(src, dst, nf, op);
+        }
+        auto kp = k_plane<T, EP, S1, S2, Op>;
+        set_smem(kp, plane_smem);
+        kp<<<dim3(c.m1, nf), plane_threads, plane_smem, stream>>>(pg, src, dst, V_, tw2.p, tw3.p, op);
+        ++launches;
+    }
+
+    template <int DIM, int N, int S1, int S2, class Op>
+    void strided_ct(const V* src, V* dst, int nf, const Op& op)
+    {
+        constexpr int E = F32 ? 16 : 8;
+        constexpr int NT = N * WCT / E;
+        auto k = k_strided_ct<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
+        const size_t smem = std::max(sizeof(V) * (size_t)(N * WCT + N), (size_t)4096);
+        set_smem(k, smem);
+        const int outer = DIM == 1 ? c.m1 : c.m2;
+        k<<<dim3(outer * (c.m3 / WCT), nf), NT, smem, stream>>>(c.m2, c.m3, src, dst, V_, DIM == 1 ? tw2.p : tw1.p, op);
+        ++launches;
+    }
+
+    bool strided_is_ct(int n) const { return c.m3 % WCT == 0 && (n == 32 || n == 64 || n == 128); }
+
+    template <int DIM, int S1, int S2, class Op>
+    void strided(const V* src, V* dst, int nf, const Op& op)
+    {
+        const int n = DIM == 1 ? c.m2 : c.m1;
+        if constexpr (DIM == 0 || !F32) {
+            if (strided_is_ct(n)) {
+                if (n == 128) return strided_ct<DIM, 128, S1, S2>(src, dst, nf, op);
+                if (n == 64) return strided_ct<DIM, 64, S1, S2>(src, dst, nf, op);
+                return strided_ct<DIM, 32, S1, S2>(src, dst, nf, op);
+            }
+        }
+        const LineGeom& g = DIM == 1 ? gy : gx;
+        auto k = k_strided<T, EL, DIM, S1, S2, Op>;
+        const size_t smem = DIM == 1 ? y_smem : x_smem;
+        set_smem(k, smem);
+        const int outer = DIM == 1 ? c.m1 : c.m2;
+        k<<<dim3(outer * (c.m3 / g.W), nf), DIM == 1 ? y_threads : x_threads, smem, stream>>>(g, src, dst, V_,
+                                                                                            DIM == 1 ? tw2.p : tw1.p, op);
+        ++launches;
+    }
+
+    template <int S1, int S2, class Op>
+    void zline(const V* src, V* dst, int nf, const Op& op)
+    {
+        if constexpr (!F32) {
+            if (c.m3 == 128 && (c.m1 * c.m2) % 16 == 0) {
+                constexpr int N = 128, BR = 16, E = 8, NT = BR * N / E;
+                auto k = k_zline_ct<T, N, BR, RMAX, NT, E, S1, S2, Op>;
+                const size_t smem = sizeof(V) * (size_t)(BR * (N + 1) + N);
+                set_smem(k, smem);
+                k<<<dim3(c.m1 * c.m2 / BR, nf), NT, smem, stream>>>(c.m2, src, dst, V_, tw3.p, op);
+                ++launches;
+                return;
+            }
+        }
+        auto k = k_zline<T, EL, S1, S2, Op>;
+        set_smem(k, z_smem);
+        k<<<dim3(c.m1 * c.m2 / gz.B, nf), z_threads, z_smem, stream>>>(gz, src, dst, V_, tw3.p, op);
+        ++launches;
+    }
+
+    // Batched in-place (or out-of-place from per-field sources) 3-D FFT of nf
+    // contiguous fields of dst.  src[f] (optional) gives the input of field f.
     template <int S>
     void fft3(V* dst, int nf, const V* const* src = nullptr)
     {
         using OpLoad = OpLoadN<T>;
+        if (nf > 16) throw std::runtime_error("fft3: too many fields in one batch");
         OpLoad in{};
-        for (int f = 0; f < nf && f < 16; ++f) in.s[f] = src ? src[f] : dst + (size_t)f * V_;
+        for (int f = 0; f < nf; ++f) in.s[f] = src ? src[f] : dst + (size_t)f * V_;
         in.fs = V_;
         OpLoad self{};
-        for (int f = 0; f < nf && f < 16; ++f) self.s[f] = dst + (size_t)f * V_;
+        for (int f = 0; f < nf; ++f) self.s[f] = dst + (size_t)f * V_;
         self.fs = V_;
-        if (nf > 16) throw std::runtime_error("fft3: too many fields in one batch");
         if (plane_ok) {
-            auto kp = k_plane<T, EP, 0, S, OpLoad>;
-            set_smem(kp, plane_smem);
-            kp<<<dim3(c.m1, nf), plane_threads, plane_smem, stream>>>(pg, nullptr, dst, V_, tw2.p, tw3.p, in);
+            plane<0, S>(nullptr, dst, nf, in);
         } else {
-            auto kz = k_zline<T, EL, 0, S, OpLoad>;
-            set_smem(kz, z_smem);
-            kz<<<dim3(c.m1 * c.m2 / gz.B, nf), z_threads, z_smem, stream>>>(gz, nullptr, dst, V_, tw3.p, in);
-            auto ky_ = k_strided<T, EL, 1, 0, S, OpLoad>;
-            set_smem(ky_, y_smem);
-            ky_<<<dim3(c.m1 * (c.m3 / gy.W), nf), y_threads, y_smem, stream>>>(gy, nullptr, dst, V_, tw2.p, self);
-            ++launches;
+            zline<0, S>(nullptr, dst, nf, in);
+            strided<1, 0, S>(nullptr, dst, nf, self);
         }
-        auto kx_ = k_strided<T, EL, 0, 0, S, OpLoad>;
-        set_smem(kx_, x_smem);
-        kx_<<<dim3(c.m2 * (c.m3 / gx.W), nf), x_threads, x_smem, stream>>>(gx, nullptr, dst, V_, tw1.p, self);
-        launches += 2;
+        strided<0, 0, S>(nullptr, dst, nf, self);
     }
 
     // Real-space pass of one segment: [inverse S1] op [forward S2] with the
     // propagator op.  Plane pass when the plane fits, else y / z-line / y.
-    template <int S1, int S2, int KIND>
-    void seg_pass(const V* src, V* dst, const OpProp<T, KIND>& op)
+    static const char* kind_name(int k)
     {
-        using OpLoadOne = ftsp::OpLoadOne<T>;
-        if (plane_ok) {
-            auto kp = k_plane<T, EP, S1, S2, OpProp<T, KIND>>;
-            set_smem(kp, plane_smem);
-            kp<<<dim3(c.m1, 1), plane_threads, plane_smem, stream>>>(pg, src, dst, V_, tw2.p, tw3.p, op);
-            ++launches;
-            return;
-        }
-        if (S1 != 0) {   // y-lines of the inverse, in place on src
-            auto ky_ = k_strided<T, EL, 1, 0, S1, OpLoadOne>;
-            set_smem(ky_, y_smem);
-            ky_<<<dim3(c.m1 * (c.m3 / gy.W), 1), y_threads, y_smem, stream>>>(gy, nullptr, const_cast<V*>(src), V_, tw2.p, OpLoadOne{src});
-            ++launches;
-        }
-        auto kz_ = k_zline<T, EL, S1, S2, OpProp<T, KIND>>;
-        set_smem(kz_, z_smem);
-        kz_<<<dim3(c.m1 * c.m2 / gz.B, 1), z_threads, z_smem, stream>>>(gz, src, dst, V_, tw3.p, op);
-        ++launches;
-        if (S2 != 0) {   // y-lines of the forward transform, in place on dst
-            auto ky_ = k_strided<T, EL, 1, 0, S2, OpLoadOne>;
-            set_smem(ky_, y_smem);
-            ky_<<<dim3(c.m1 * (c.m3 / gy.W), 1), y_threads, y_smem, stream>>>(gy, nullptr, dst, V_, tw2.p, OpLoadOne{dst});
-            ++launches;
+        static const char* n[] = {"fwd_start", "fwd_mid", "fwd_last", "fwd_single", "bwd_start", "bwd_mid", "bwd_last", "bwd_single"};
+        return n[k];
+    }
+    // algorithmic bytes of one real-space segment pass (complex elements moved per grid point)
+    static int seg_units(int k, bool charged)
+    {
+        switch (k) {
+        case FWD_START: return 3;                      // E, q store, G
+        case FWD_MID: return 4;                        // H, E, q store, G
+        case FWD_LAST: return 3;                       // H, E, q store
+        case FWD_SINGLE: return 2;                     // E, q store
+        case BWD_START: return 5 + (charged ? 2 : 0);  // E, qF, rho rmw, (rho_c rmw), G
+        case BWD_MID: return 6 + (charged ? 2 : 0);    // H, qF, E, rho rmw, (rho_c rmw), G
+        case BWD_LAST: return 4 + (charged ? 2 : 0);   // H, qF, rho rmw, (rho_c rmw)
+        default: return 3 + (charged ? 2 : 0);         // qF, rho rmw, (rho_c rmw)
         }
     }
 
-    int seg_pass_ctas() const { return plane_ok ? c.m1 : c.m1 * c.m2 / gz.B; }
-    int x_ctas() const { return c.m2 * (c.m3 / gx.W); }
+    template <int S1, int S2, int KIND>
+    void seg_pass(const V* src, V* dst, const OpProp<T, KIND>& op)
+    {
+        cudaEvent_t ev = prof_begin();
+        seg_pass_launch<S1, S2, KIND>(src, dst, op);
+        prof_end(ev, std::string(plane_ok ? "plane_" : "zline_") + kind_name(KIND),
+                 (double)seg_units(KIND, op.rho_charge != nullptr) * sizeof(V) * (double)V_);
+    }
+
+    template <int S1, int S2, int KIND>
+    void seg_pass_launch(const V* src, V* dst, const OpProp<T, KIND>& op)
+    {
+        using OpLoadOne = ftsp::OpLoadOne<T>;
+        if (plane_ok) {
+            plane<S1, S2>(src, dst, 1, op);
+            return;
+        }
+        if (S1 != 0) strided<1, 0, S1>(nullptr, const_cast<V*>(src), 1, OpLoadOne{src});   // y-lines, in place
+        zline<S1, S2>(src, dst, 1, op);
+        if (S2 != 0) strided<1, 0, S2>(nullptr, dst, 1, OpLoadOne{dst});                    // y-lines, in place
+    }
+
+    int seg_pass_ctas() const
+    {
+        if (plane_ok) return c.m1;
+        if (!F32 && c.m3 == 128 && (c.m1 * c.m2) % 16 == 0) return c.m1 * c.m2 / 16;
+        return c.m1 * c.m2 / gz.B;
+    }
+    int x_ctas() const { return c.m2 * (c.m3 / (strided_is_ct(c.m1) ? WCT : gx.W)); }
 
     template <int S1, int S2, bool FWD, bool STRESS>
     void bond_pass(const V* src, V* dst, const OpBond<T, FWD, STRESS>& op)
     {
-        auto kx_ = k_strided<T, EL, 0, S1, S2, OpBond<T, FWD, STRESS>>;
-        set_smem(kx_, x_smem);
-        kx_<<<dim3(x_ctas(), 1), x_threads, x_smem, stream>>>(gx, src, dst, V_, tw1.p, op);
-        ++launches;
+        cudaEvent_t ev = prof_begin();
+        strided<0, S1, S2>(src, dst, 1, op);
+        // G in, H out, plus the stored/read forward spectrum when the stress is on
+        const bool extra = FWD ? op.Fstore != nullptr : STRESS;
+        prof_end(ev, std::string("bond_") + (FWD ? "fwd" : "bwd") + (extra ? (FWD ? "_storeF" : "_stress") : ""),
+                 (double)(2 + (extra ? 1 : 0)) * sizeof(V) * (double)V_);
     }
 
     // ---- chain propagators of one species; densities accumulate into dB ----
@@ -1273,34 +1485,36 @@ struct Engine : EngineBase {
     }
 
     // ---- API ----
-    void to_device_field(V* dst, const double* src, size_t count)
-    {
-        if (sizeof(T) == 8) {
-            FTSP_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * 2 * count, cudaMemcpyHostToDevice, stream));
-        } else {
-            std::vector<V> tmp(count);
-            for (size_t i = 0; i < count; ++i) {
-                tmp[i].x = (T)src[2 * i];
-                tmp[i].y = (T)src[2 * i + 1];
-            }
-            FTSP_CUDA(cudaMemcpyAsync(dst, tmp.data(), sizeof(V) * count, cudaMemcpyHostToDevice, stream));
-            FTSP_CUDA(cudaStreamSynchronize(stream));
-        }
-    }
+    Buf<double2> stage;   // FP64 host fields land here, then convert on the device
 
     void set_fields(const double* om, const double* ps) override
     {
-        if (c.nm > 0) to_device_field(omega.p, om, (size_t)c.nm * V_);
-        to_device_field(psi.p, ps, V_);
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        if (sizeof(T) == 8) {
+            if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(omega.p, om, sizeof(double2) * nm * Vn, cudaMemcpyHostToDevice, stream));
+            FTSP_CUDA(cudaMemcpyAsync(psi.p, ps, sizeof(double2) * Vn, cudaMemcpyHostToDevice, stream));
+        } else {
+            if (!stage.p) stage.alloc((size_t)(nm + 1) * Vn);
+            if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(stage.p, om, sizeof(double2) * nm * Vn, cudaMemcpyHostToDevice, stream));
+            FTSP_CUDA(cudaMemcpyAsync(stage.p + (size_t)nm * Vn, ps, sizeof(double2) * Vn, cudaMemcpyHostToDevice, stream));
+            const double2* s = stage.p;
+            V* o = omega.p;
+            V* p = psi.p;
+            foreach(Vn, [=] __device__(size_t i) {
+                for (int a = 0; a < nm; ++a) o[(size_t)a * Vn + i] = from_d<V>(s[(size_t)a * Vn + i]);
+                p[i] = from_d<V>(s[(size_t)nm * Vn + i]);
+            });
+        }
         if (c.elec) {
             const V* p = psi.p;
-            reduce<2>(V_, [=] __device__(size_t i, double* acc) {
+            reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
                 acc[0] += (double)p[i].x;
                 acc[1] += (double)p[i].y;
             }, reinterpret_cast<double*>(&ds->mean_psi));
             remove_mean(psi.p, &ds->mean_psi);
         } else {
-            FTSP_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(V) * V_, stream));
+            FTSP_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(V) * Vn, stream));
         }
         FTSP_CUDA(cudaStreamSynchronize(stream));
     }
@@ -1468,228 +1682,8 @@ struct Engine : EngineBase {
     }
 };
 
-static HostCfg make_cfg(const ftsp_config* in)
-{
-    HostCfg c{};
-    c.m1 = in->m1; c.m2 = in->m2; c.m3 = in->m3;
-    if (c.m1 <= 0 || c.m2 <= 0 || c.m3 <= 0) throw std::runtime_error("invalid mesh");
-    c.V = (size_t)c.m1 * c.m2 * c.m3;
-    c.L[0] = in->L1; c.L[1] = in->L2; c.L[2] = in->L3;
-    c.volume = in->L1 * in->L2 * in->L3;
-    c.dV = in->dV; c.a = in->a; c.lB = in->lB; c.dt = in->dt; c.lpsi = in->lambda_psi;
-    c.elec = in->lB > 0.0;
-    c.M = in->M; c.nm = in->n_modes;
-    if (c.M < 1 || c.M > MAXM) throw std::runtime_error("monomer type count out of range (1..8)");
-    if (c.nm < 0 || c.nm > MAXMODE) throw std::runtime_error("active mode count out of range (0..8)");
-    for (int a = 0; a < c.nm; ++a) {
-        c.coeff.push_back(in->mode_coeff[a]);
-        c.lambda.push_back(in->mode_lambda[a]);
-        c.gamma.push_back(make_double2(in->mode_gamma[2 * a], in->mode_gamma[2 * a + 1]));
-        for (int al = 0; al < c.M; ++al) c.O.push_back(in->mode_O[a * c.M + al]);
-    }
-    if (in->n_species < 1 || in->n_species > MAXSP) throw std::runtime_error("polymer species count out of range (1..16)");
-    if (in->n_ions < 0 || in->n_ions > MAXION) throw std::runtime_error("ion species count out of range (0..16)");
-    int off = 0;
-    for (int s = 0; s < in->n_species; ++s) {
-        Species sp{};
-        sp.nc = in->num_chains[s];
-        sp.N = in->N[s];
-        if (sp.N < 1) throw std::runtime_error("species with N < 1");
-        for (int t = 0; t < sp.N; ++t) {
-            const int ty = in->seg_type[off + t];
-            if (ty < 0 || ty >= c.M) throw std::runtime_error("segment monomer type out of range");
-            sp.type.push_back(ty);
-            sp.charge.push_back(in->seg_charge[off + t]);
-            sp.bond.push_back(in->seg_bond[off + t]);
-        }
-        off += sp.N;
-        for (int t = 0; t < sp.N; ++t) {
-            const double z = c.elec ? sp.charge[t] : 0.0;
-            int k = -1;
-            for (size_t q = 0; q < c.cls.size(); ++q)
-                if (c.cls[q].type == sp.type[t] && c.cls[q].z == z) k = (int)q;
-            if (k < 0) {
-                c.cls.push_back(Cls{sp.type[t], z});
-                k = (int)c.cls.size() - 1;
-            }
-            sp.cls.push_back(k);
-        }
-        for (int t = 0; t + 1 < sp.N; ++t) {
-            int k = -1;
-            for (size_t q = 0; q < c.bond_lengths.size(); ++q)
-                if (c.bond_lengths[q] == sp.bond[t]) k = (int)q;
-            if (k < 0) {
-                c.bond_lengths.push_back(sp.bond[t]);
-                k = (int)c.bond_lengths.size() - 1;
-            }
-            sp.bcls.push_back(k);
-        }
-        c.sp.push_back(sp);
-    }
-    for (int j = 0; j < in->n_ions; ++j) c.ions.push_back(Ion{in->ion_valence[j], in->ion_count[j], in->ion_smear[j]});
-    c.self_pressure = in->self_pressure;
-    c.stress_mask = in->stress_mask & 63;
-    c.iso = in->isotropic_pressure ? 1 : 0;
-    c.noise = in->noise != 0;
-    c.seed = in->seed;
-    c.precision = in->precision;
-    c.scheme = in->scheme;
-    c.device = in->device;
-    if (c.record_len() > 128) throw std::runtime_error("observable record too long");
-    return c;
-}
+
+EngineBase* make_engine_f32(const HostCfg& c);
+EngineBase* make_engine_f64(const HostCfg& c);
 
 }  // namespace ftsp
-
-// ---------------------------------------------------------------------------
-// C ABI
-// ---------------------------------------------------------------------------
-struct ftsp_handle {
-    std::unique_ptr<ftsp::EngineBase> eng;
-    std::string err;
-};
-
-static thread_local std::string g_create_error;
-
-#define FTSP_GUARD(h, body)                                      \
-    do {                                                         \
-        if (!(h) || !(h)->eng) return FTSP_ERROR;                \
-        try {                                                    \
-            body;                                                \
-        } catch (const std::exception& e_) {                     \
-            (h)->err = e_.what();                                \
-            return FTSP_ERROR;                                   \
-        }                                                        \
-    } while (0)
-
-extern "C" {
-
-int ftsp_create(const ftsp_config* cfg, ftsp_handle** out)
-{
-    if (!cfg || !out) return FTSP_ERROR;
-    *out = nullptr;
-    try {
-        ftsp::HostCfg c = ftsp::make_cfg(cfg);
-        auto* h = new ftsp_handle();
-        if (c.precision == FTSP_FP32) h->eng.reset(new ftsp::Engine<float>(c));
-        else h->eng.reset(new ftsp::Engine<double>(c));
-        *out = h;
-        return FTSP_OK;
-    } catch (const std::exception& e) {
-        g_create_error = e.what();
-        return FTSP_ERROR;
-    }
-}
-
-int ftsp_destroy(ftsp_handle* h)
-{
-    if (!h) return FTSP_ERROR;
-    try {
-        h->eng.reset();
-    } catch (...) {
-    }
-    delete h;
-    return FTSP_OK;
-}
-
-const char* ftsp_last_error(const ftsp_handle* h)
-{
-    if (!h) return g_create_error.c_str();
-    return h->err.c_str();
-}
-
-int ftsp_set_stream(ftsp_handle* h, void* s)
-{
-    FTSP_GUARD(h, h->eng->stream = static_cast<cudaStream_t>(s));
-    return FTSP_OK;
-}
-
-int ftsp_set_fields(ftsp_handle* h, const double* omega, const double* psi)
-{
-    if (!psi) return FTSP_ERROR;
-    FTSP_GUARD(h, h->eng->set_fields(omega, psi));
-    return FTSP_OK;
-}
-
-int ftsp_get_field(ftsp_handle* h, const char* name, double* out, long long* count)
-{
-    long long n = -1;
-    FTSP_GUARD(h, n = h->eng->get_field(name ? name : "", out));
-    if (count) *count = n;
-    if (n < 0) {
-        h->err = std::string("unknown field ") + (name ? name : "");
-        return FTSP_ERROR;
-    }
-    return FTSP_OK;
-}
-
-int ftsp_compute_densities(ftsp_handle* h, int which, double* Q_out)
-{
-    FTSP_GUARD(h, h->eng->compute_densities(which ? 1 : 0, Q_out));
-    for (size_t s = 0; s < h->eng->c.sp.size(); ++s)
-        if (Q_out && !(std::isfinite(Q_out[2 * s]) && std::isfinite(Q_out[2 * s + 1]))) return FTSP_NONFINITE;
-    return FTSP_OK;
-}
-
-int ftsp_record_length(const ftsp_handle* h)
-{
-    if (!h || !h->eng) return -1;
-    return h->eng->c.record_len();
-}
-
-int ftsp_measure(ftsp_handle* h, int which, double* record)
-{
-    FTSP_GUARD(h, h->eng->measure(which ? 1 : 0, record));
-    if (record)
-        for (int i = 0; i < 2 * h->eng->c.record_len(); ++i)
-            if (!std::isfinite(record[i])) return FTSP_NONFINITE;
-    return FTSP_OK;
-}
-
-int ftsp_set_noise(ftsp_handle* h, const double* eta)
-{
-    if (!eta) return FTSP_ERROR;
-    FTSP_GUARD(h, h->eng->set_noise(eta));
-    return FTSP_OK;
-}
-
-int ftsp_set_seed(ftsp_handle* h, unsigned long long seed)
-{
-    FTSP_GUARD(h, h->eng->c.seed = seed);
-    return FTSP_OK;
-}
-
-int ftsp_step(ftsp_handle* h, double* Q_bar, double* record, double* drift_max)
-{
-    int st = FTSP_ERROR;
-    FTSP_GUARD(h, st = h->eng->step(Q_bar, record, drift_max, true));
-    return st;
-}
-
-int ftsp_step_async(ftsp_handle* h)
-{
-    FTSP_GUARD(h, h->eng->step(nullptr, nullptr, nullptr, false));
-    return FTSP_OK;
-}
-
-int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max)
-{
-    int st = FTSP_ERROR;
-    FTSP_GUARD(h, st = h->eng->read_status(record, drift_max));
-    return st;
-}
-
-int ftsp_state_views(ftsp_handle* h, ftsp_views* v)
-{
-    if (!v) return FTSP_ERROR;
-    FTSP_GUARD(h, h->eng->views(v));
-    return FTSP_OK;
-}
-
-long long ftsp_last_launch_count(const ftsp_handle* h)
-{
-    if (!h || !h->eng) return -1;
-    return h->eng->launches;
-}
-
-}  // extern "C"

@@ -12,8 +12,11 @@
 // butterflies in registers, the block synchronises, then the outputs are
 // written.  Twiddles come from a table w_n^j = exp(-2*pi*i*j/n) held in
 // shared memory (computed on the host in long double), conjugated for S = +1.
-// Radices 2, 3, 4, 5 and 8 are compiled; the per-size factorisation is a
-// runtime plan (FftPlan1) so one kernel serves every 2/3/5-smooth length.
+// Radices 2, 3, 4, 5, 8 and 16 are compiled; the per-size factorisation is
+// a runtime plan (FftPlan1) so one kernel serves every 2/3/5-smooth length.
+// Index arithmetic uses precomputed magic-number division (FastDiv) instead
+// of hardware-emulated integer division, and a thread recomputes its
+// butterfly indices after the barrier instead of keeping them live.
 //
 // Conventions follow cuFFT's: S = -1 forward, S = +1 inverse, unnormalised.
 #pragma once
@@ -124,6 +127,45 @@ template <int S, typename V> __device__ __forceinline__ void dft8(V* u)
     }
 }
 
+// 16 = 4 x 4: DFT4 over the stride-4 sub-sequences, twiddles W16^(j*k),
+// DFT4 across them; outputs in natural order.
+template <int S, typename V> __device__ __forceinline__ void dft16(V* u)
+{
+    using R = typename RealOf<V>::type;
+    const R c1 = R(0.92387953251128675612818318939678829);   // cos(pi/8)
+    const R s1 = R(0.38268343236508977172845998403039887);   // sin(pi/8)
+    const R r2 = R(0.70710678118654752440084436210484904);   // 1/sqrt(2)
+    V a[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        a[j][0] = u[j];
+        a[j][1] = u[j + 4];
+        a[j][2] = u[j + 8];
+        a[j][3] = u[j + 12];
+        dft4<S>(a[j]);
+    }
+    // a[j][k] *= exp(S*2*pi*i*j*k/16) for j, k in 1..3
+    auto rot = [](V z, R c, R sn) { return mkc<V>(z.x * c - S * z.y * sn, z.y * c + S * z.x * sn); };
+    a[1][1] = rot(a[1][1], c1, s1);
+    a[1][2] = rot(a[1][2], r2, r2);
+    a[1][3] = rot(a[1][3], s1, c1);
+    a[2][1] = rot(a[2][1], r2, r2);
+    a[2][2] = mul_si<S>(a[2][2]);
+    a[2][3] = rot(a[2][3], -r2, r2);
+    a[3][1] = rot(a[3][1], s1, c1);
+    a[3][2] = rot(a[3][2], -r2, r2);
+    a[3][3] = rot(a[3][3], -c1, -s1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        V b[4] = {a[0][k], a[1][k], a[2][k], a[3][k]};
+        dft4<S>(b);
+        u[k] = b[0];
+        u[k + 4] = b[1];
+        u[k + 8] = b[2];
+        u[k + 12] = b[3];
+    }
+}
+
 template <int S, int R, typename V> __device__ __forceinline__ void dftR(V* u)
 {
     if constexpr (R == 2) dft2<S>(u);
@@ -131,13 +173,36 @@ template <int S, int R, typename V> __device__ __forceinline__ void dftR(V* u)
     else if constexpr (R == 4) dft4<S>(u);
     else if constexpr (R == 5) dft5<S>(u);
     else if constexpr (R == 8) dft8<S>(u);
+    else if constexpr (R == 16) dft16<S>(u);
 }
 
-// Runtime factorisation of one transform length.
+// Magic-number division for 0 <= n < 2^31 (Granlund & Montgomery, PLDI'94):
+// q = (umulhi(n, m) + n) >> s with s = ceil(log2 d), m = 2^32 (2^s - d)/d + 1.
+struct FastDiv {
+    unsigned d, m, s;
+};
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return (__umulhi(n, f.m) + n) >> f.s; }
+inline FastDiv make_fastdiv(unsigned d)
+{
+    FastDiv f{d, 0u, 0u};
+    if (d <= 1) return f;
+    unsigned l = 0;
+    while ((1u << l) < d) ++l;
+    f.m = (unsigned)(((1ull << 32) * ((1ull << l) - d)) / d + 1ull);
+    f.s = l;
+    return f;
+}
+
+// Runtime factorisation of one transform length: radices, the span (product
+// of the earlier radices) before each stage with its FastDiv, and the twiddle
+// index step n / (R * span).
 struct FftPlan1 {
     int n;
     int nst;
-    int rad[12];
+    int rad[8];
+    int span[8];
+    int tstep[8];
+    FastDiv fspan[8];
 };
 
 template <int S, typename V> __device__ __forceinline__ V twiddle(const V* tw, int idx)
@@ -148,62 +213,68 @@ template <int S, typename V> __device__ __forceinline__ V twiddle(const V* tw, i
 }
 
 // One radix-R stage over a tile.  E bounds the elements any thread touches:
-// the caller guarantees B*n <= E*blockDim.x.
+// the caller guarantees B*n <= E*blockDim.x.  Butterfly idx maps to line
+// b = idx mod B and butterfly i = idx div B of that line.
 template <typename V, int S, int R, int E>
-__device__ __forceinline__ void fft_stage(V* tile, const V* __restrict__ tw, int n, int B, int js, int bs, int span)
+__device__ __noinline__ void fft_stage(V* tile, const V* __restrict__ tw, unsigned n, unsigned B, const FastDiv& fB,
+                                          int js, int bs, unsigned span, const FastDiv& fspan, unsigned tstep)
 {
     constexpr int NB = (E + R - 1) / R;
-    const int m = n / R;
-    const int total = B * m;
-    const int tstep = n / (R * span);
+    const unsigned m = n / R;
+    const unsigned total = B * m;
     V u[NB][R];
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const unsigned idx = threadIdx.x + q * blockDim.x;
         if (idx < total) {
-            const int b = idx % B, i = idx / B;
-            const V* src = tile + i * js + b * bs;
+            const unsigned i = fdiv(idx, fB), b = idx - i * B;
+            const V* src = tile + (int)i * js + (int)b * bs;
 #pragma unroll
-            for (int t = 0; t < R; ++t) u[q][t] = src[t * m * js];
+            for (int t = 0; t < R; ++t) u[q][t] = src[t * (int)m * js];
         }
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const unsigned idx = threadIdx.x + q * blockDim.x;
         if (idx < total) {
-            const int b = idx % B, i = idx / B;
-            const int k = i % span;
+            const unsigned i = fdiv(idx, fB), b = idx - i * B;
+            const unsigned kq = fdiv(i, fspan), k = i - kq * span;
             if (k) {
-                const int step = k * tstep;
+                const unsigned step = k * tstep;
 #pragma unroll
                 for (int t = 1; t < R; ++t) u[q][t] = cmul(u[q][t], twiddle<S>(tw, t * step));
             }
             dftR<S, R>(u[q]);
-            V* dst = tile + ((i - k) * R + k) * js + b * bs;
+            V* dst = tile + (int)(kq * span * R + k) * js + (int)b * bs;
 #pragma unroll
-            for (int t = 0; t < R; ++t) dst[t * span * js] = u[q][t];
+            for (int t = 0; t < R; ++t) dst[t * (int)span * js] = u[q][t];
         }
     }
     __syncthreads();
 }
 
-// Full transform of a tile (caller has synchronised after filling it).
+// Full transform of a tile (caller has synchronised after filling it).  The
+// plan lives in device memory (uniform loads): indexing a plan held in the
+// kernel's parameter block by stage would force a local-memory copy of it.
 template <typename V, int S, int E>
-__device__ __forceinline__ void fft_tile(V* tile, const V* __restrict__ tw, const FftPlan1& p, int B, int js, int bs)
+__device__ __forceinline__ void fft_tile(V* tile, const V* __restrict__ tw, const FftPlan1* __restrict__ p, unsigned B,
+                                         const FastDiv& fB, int js, int bs)
 {
-    int span = 1;
-    for (int st = 0; st < p.nst; ++st) {
-        const int R = p.rad[st];
-        switch (R) {
-        case 8: fft_stage<V, S, 8, E>(tile, tw, p.n, B, js, bs, span); break;
-        case 4: fft_stage<V, S, 4, E>(tile, tw, p.n, B, js, bs, span); break;
-        case 2: fft_stage<V, S, 2, E>(tile, tw, p.n, B, js, bs, span); break;
-        case 3: fft_stage<V, S, 3, E>(tile, tw, p.n, B, js, bs, span); break;
-        case 5: fft_stage<V, S, 5, E>(tile, tw, p.n, B, js, bs, span); break;
+    const int nst = p->nst;
+    const unsigned n = p->n;
+    for (int st = 0; st < nst; ++st) {
+        const unsigned span = p->span[st], tstep = p->tstep[st];
+        const FastDiv fs = p->fspan[st];
+        switch (p->rad[st]) {
+        case 16: if constexpr (E >= 16) fft_stage<V, S, 16, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 8: fft_stage<V, S, 8, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 4: fft_stage<V, S, 4, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 2: fft_stage<V, S, 2, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 3: fft_stage<V, S, 3, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 5: fft_stage<V, S, 5, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
         default: break;
         }
-        span *= R;
     }
 }
 
@@ -211,6 +282,123 @@ template <typename V>
 __device__ __forceinline__ void load_twiddles(V* dst, const V* __restrict__ src, int n)
 {
     for (int j = threadIdx.x; j < n; j += blockDim.x) dst[j] = src[j];
+}
+
+}  // namespace ftsp
+
+namespace ftsp {
+
+// ---------------------------------------------------------------------------
+// Compile-time transforms for the production lengths.  Length, batch,
+// strides, thread count and the radix plan are constants, the stages are
+// unrolled, and every index is computed with constant divisors.  The plan is
+// the runtime planner's: the power-of-two part in the fewest stages of radix
+// <= RMAX spread evenly, then 3s and 5s.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ct_p2(int n)
+{
+    int p = 0;
+    while (n % 2 == 0) {
+        n /= 2;
+        ++p;
+    }
+    return p;
+}
+__host__ __device__ constexpr int ct_lg(int r)
+{
+    int l = 0;
+    while ((1 << l) < r) ++l;
+    return l;
+}
+__host__ __device__ constexpr int ct_nst(int n, int rmax)
+{
+    const int p2 = ct_p2(n), bits = ct_lg(rmax);
+    int r = n >> p2, nst = (p2 + bits - 1) / bits;
+    while (r % 3 == 0) { r /= 3; ++nst; }
+    while (r % 5 == 0) { r /= 5; ++nst; }
+    return nst;
+}
+__host__ __device__ constexpr int ct_rad(int n, int rmax, int st)
+{
+    const int p2 = ct_p2(n), bits = ct_lg(rmax);
+    const int nst2 = (p2 + bits - 1) / bits;
+    int left = p2;
+    for (int s = 0; s < nst2; ++s) {
+        const int b = (left + (nst2 - s) - 1) / (nst2 - s);
+        if (s == st) return 1 << b;
+        left -= b;
+    }
+    int r = n >> p2, s = nst2;
+    while (r % 3 == 0) {
+        if (s == st) return 3;
+        r /= 3;
+        ++s;
+    }
+    while (r % 5 == 0) {
+        if (s == st) return 5;
+        r /= 5;
+        ++s;
+    }
+    return 1;
+}
+__host__ __device__ constexpr int ct_span(int n, int rmax, int st)
+{
+    int s = 1;
+    for (int k = 0; k < st; ++k) s *= ct_rad(n, rmax, k);
+    return s;
+}
+
+// One stage: B lines of length N, element (j, b) at tile[j*JS + b*BS],
+// NT threads, E elements per thread at most (B*N <= E*NT).
+template <typename V, int S, int N, int RMAX, int B, int JS, int BS, int NT, int E, int ST>
+__device__ __forceinline__ void ct_stage(V* tile, const V* __restrict__ tw)
+{
+    constexpr int R = ct_rad(N, RMAX, ST);
+    constexpr int SPAN = ct_span(N, RMAX, ST);
+    constexpr int M = N / R;
+    constexpr int TOTAL = B * M;
+    constexpr int TSTEP = N / (R * SPAN);
+    constexpr int NB = (TOTAL + NT - 1) / NT;
+    static_assert(NB * R <= E + R, "too many elements per thread");
+    V u[NB][R];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const unsigned idx = threadIdx.x + q * NT;
+        if (TOTAL % NT == 0 || idx < (unsigned)TOTAL) {
+            const unsigned i = idx / B, b = idx % B;
+            const V* src = tile + i * JS + b * BS;
+#pragma unroll
+            for (int t = 0; t < R; ++t) u[q][t] = src[t * M * JS];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const unsigned idx = threadIdx.x + q * NT;
+        if (TOTAL % NT == 0 || idx < (unsigned)TOTAL) {
+            const unsigned i = idx / B, b = idx % B;
+            const unsigned k = i % SPAN, kq = i / SPAN;
+            if (SPAN > 1 && k) {
+                const unsigned step = k * TSTEP;
+#pragma unroll
+                for (int t = 1; t < R; ++t) u[q][t] = cmul(u[q][t], twiddle<S>(tw, t * step));
+            }
+            dftR<S, R>(u[q]);
+            V* dst = tile + (kq * SPAN * R + k) * JS + b * BS;
+#pragma unroll
+            for (int t = 0; t < R; ++t) dst[t * SPAN * JS] = u[q][t];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename V, int S, int N, int RMAX, int B, int JS, int BS, int NT, int E, int ST = 0>
+__device__ __forceinline__ void ct_fft(V* tile, const V* __restrict__ tw)
+{
+    if constexpr (ST < ct_nst(N, RMAX)) {
+        ct_stage<V, S, N, RMAX, B, JS, BS, NT, E, ST>(tile, tw);
+        ct_fft<V, S, N, RMAX, B, JS, BS, NT, E, ST + 1>(tile, tw);
+    }
 }
 
 }  // namespace ftsp

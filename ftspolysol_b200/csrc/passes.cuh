@@ -24,7 +24,9 @@ namespace ftsp {
 struct PlaneGeom {
     int m1, m2, m3;
     int P;                 // shared-memory pitch of a plane row (m3 + 1)
-    FftPlan1 py, pz;
+    const FftPlan1* py;    // device-memory plans of the y and z transforms
+    const FftPlan1* pz;
+    FastDiv fm2, fm3;
 };
 
 struct LineGeom {
@@ -33,7 +35,8 @@ struct LineGeom {
     int W;                 // z-columns per tile (strided passes)
     int B;                 // rows per tile (z-line pass)
     int P;                 // shared-memory pitch
-    FftPlan1 p;
+    const FftPlan1* p;     // device-memory plan of the transform
+    FastDiv fW, fB, fm2, fm3;
 };
 
 // ---- block reductions (deterministic: fixed shuffle/smem order) ----
@@ -70,7 +73,7 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* scratch)
 // Shared memory: tile[m2][P] + twiddles(m2) + twiddles(m3).
 // ---------------------------------------------------------------------------
 template <typename T, int E, int S1, int S2, class Op>
-__global__ void __launch_bounds__(512) k_plane(PlaneGeom g, const cplx<T>* src, cplx<T>* dst,
+__global__ void __launch_bounds__(1024, 1) k_plane(PlaneGeom g, const cplx<T>* src, cplx<T>* dst,
                                                 size_t fstride, const cplx<T>* __restrict__ twy,
                                                 const cplx<T>* __restrict__ twz, Op op)
 {
@@ -88,29 +91,41 @@ __global__ void __launch_bounds__(512) k_plane(PlaneGeom g, const cplx<T>* src, 
         load_twiddles(stz, twz, g.m3);
     }
     if (S1 != 0) {
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int y = e / g.m3, z = e - y * g.m3;
-            tile[y * g.P + z] = src[base + e];
+        for (int e0 = threadIdx.x; e0 < ne; e0 += 4 * blockDim.x) {
+            V v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < ne) v[u] = src[base + e];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < ne) {
+                    const int y = fdiv(e, g.fm3), z = e - y * g.m3;
+                    tile[y * g.P + z] = v[u];
+                }
+            }
         }
         __syncthreads();
-        fft_tile<V, S1, E>(tile, stz, g.pz, g.m2, 1, g.P);
-        fft_tile<V, S1, E>(tile, sty, g.py, g.m3, g.P, 1);
+        fft_tile<V, S1, E>(tile, stz, g.pz, g.m2, g.fm2, 1, g.P);
+        fft_tile<V, S1, E>(tile, sty, g.py, g.m3, g.fm3, g.P, 1);
     } else {
         __syncthreads();
     }
     op.begin();
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int y = e / g.m3, z = e - y * g.m3;
+        const int y = fdiv(e, g.fm3), z = e - y * g.m3;
         V v = S1 != 0 ? tile[y * g.P + z] : mkc<V>(T(0), T(0));
         v = op(f, x, y, z, base + e, v);
         if (S2 != 0) tile[y * g.P + z] = v;
     }
     if (S2 != 0) {
         __syncthreads();
-        fft_tile<V, S2, E>(tile, stz, g.pz, g.m2, 1, g.P);
-        fft_tile<V, S2, E>(tile, sty, g.py, g.m3, g.P, 1);
+        fft_tile<V, S2, E>(tile, stz, g.pz, g.m2, g.fm2, 1, g.P);
+        fft_tile<V, S2, E>(tile, sty, g.py, g.m3, g.fm3, g.P, 1);
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int y = e / g.m3, z = e - y * g.m3;
+            const int y = fdiv(e, g.fm3), z = e - y * g.m3;
             dst[base + e] = tile[y * g.P + z];
         }
     }
@@ -122,7 +137,7 @@ __global__ void __launch_bounds__(512) k_plane(PlaneGeom g, const cplx<T>* src, 
 // Shared memory: tile[B][P] (P = m3 + 1) + twiddles(m3).
 // ---------------------------------------------------------------------------
 template <typename T, int E, int S1, int S2, class Op>
-__global__ void __launch_bounds__(256) k_zline(LineGeom g, const cplx<T>* src, cplx<T>* dst,
+__global__ void __launch_bounds__(256, 2) k_zline(LineGeom g, const cplx<T>* src, cplx<T>* dst,
                                                 size_t fstride, const cplx<T>* __restrict__ twz, Op op)
 {
     using V = cplx<T>;
@@ -136,28 +151,28 @@ __global__ void __launch_bounds__(256) k_zline(LineGeom g, const cplx<T>* src, c
     if (S1 != 0 || S2 != 0) load_twiddles(st, twz, g.m3);
     if (S1 != 0) {
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int b = e / g.m3, z = e - b * g.m3;
+            const int b = fdiv(e, g.fm3), z = e - b * g.m3;
             tile[b * g.P + z] = src[base + e];
         }
         __syncthreads();
-        fft_tile<V, S1, E>(tile, st, g.p, g.B, 1, g.P);
+        fft_tile<V, S1, E>(tile, st, g.p, g.B, g.fB, 1, g.P);
     } else {
         __syncthreads();
     }
     op.begin();
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int b = e / g.m3, z = e - b * g.m3;
+        const int b = fdiv(e, g.fm3), z = e - b * g.m3;
         const int row = row0 + b;
-        const int x = row / g.m2, y = row - x * g.m2;
+        const int x = fdiv(row, g.fm2), y = row - x * g.m2;
         V v = S1 != 0 ? tile[b * g.P + z] : mkc<V>(T(0), T(0));
         v = op(f, x, y, z, base + e, v);
         if (S2 != 0) tile[b * g.P + z] = v;
     }
     if (S2 != 0) {
         __syncthreads();
-        fft_tile<V, S2, E>(tile, st, g.p, g.B, 1, g.P);
+        fft_tile<V, S2, E>(tile, st, g.p, g.B, g.fB, 1, g.P);
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int b = e / g.m3, z = e - b * g.m3;
+            const int b = fdiv(e, g.fm3), z = e - b * g.m3;
             dst[base + e] = tile[b * g.P + z];
         }
     }
@@ -169,7 +184,7 @@ __global__ void __launch_bounds__(256) k_zline(LineGeom g, const cplx<T>* src, c
 // Tile[n][W] (pitch W) of lines; the outer index is x for DIM 1, y for DIM 0.
 // ---------------------------------------------------------------------------
 template <typename T, int E, int DIM, int S1, int S2, class Op>
-__global__ void __launch_bounds__(256) k_strided(LineGeom g, const cplx<T>* src, cplx<T>* dst,
+__global__ void __launch_bounds__(256, 2) k_strided(LineGeom g, const cplx<T>* src, cplx<T>* dst,
                                                   size_t fstride, const cplx<T>* __restrict__ tw, Op op)
 {
     using V = cplx<T>;
@@ -186,18 +201,30 @@ __global__ void __launch_bounds__(256) k_strided(LineGeom g, const cplx<T>* src,
     const int ne = g.n * g.W;
     if (S1 != 0 || S2 != 0) load_twiddles(st, tw, g.n);
     if (S1 != 0) {
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int j = e / g.W, w = e - j * g.W;
-            tile[e] = src[base + j * lstride + w];
+        for (int e0 = threadIdx.x; e0 < ne; e0 += 4 * blockDim.x) {
+            V v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < ne) {
+                    const int j = fdiv(e, g.fW), w = e - j * g.W;
+                    v[u] = src[base + j * lstride + w];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < ne) tile[e] = v[u];
+            }
         }
         __syncthreads();
-        fft_tile<V, S1, E>(tile, st, g.p, g.W, g.W, 1);
+        fft_tile<V, S1, E>(tile, st, g.p, g.W, g.fW, g.W, 1);
     } else {
         __syncthreads();
     }
     op.begin();
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int j = e / g.W, w = e - j * g.W;
+        const int j = fdiv(e, g.fW), w = e - j * g.W;
         const int x = DIM == 1 ? outer : j;
         const int y = DIM == 1 ? j : outer;
         const size_t off = base + j * lstride + w;
@@ -207,9 +234,9 @@ __global__ void __launch_bounds__(256) k_strided(LineGeom g, const cplx<T>* src,
     }
     if (S2 != 0) {
         __syncthreads();
-        fft_tile<V, S2, E>(tile, st, g.p, g.W, g.W, 1);
+        fft_tile<V, S2, E>(tile, st, g.p, g.W, g.fW, g.W, 1);
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int j = e / g.W, w = e - j * g.W;
+            const int j = fdiv(e, g.fW), w = e - j * g.W;
             dst[base + j * lstride + w] = tile[e];
         }
     }
@@ -365,5 +392,167 @@ struct OpBond {
         }
     }
 };
+
+}  // namespace ftsp
+
+namespace ftsp {
+
+// ---------------------------------------------------------------------------
+// Compile-time specialisations of the three passes for production grids.
+// Same structure and Op interface as the runtime-plan kernels above; all
+// sizes are template constants.
+// ---------------------------------------------------------------------------
+
+// Plane pass for an m2 = m3 = N plane, NT threads, E elements per thread.
+template <typename T, int N, int RMAX, int NT, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>* dst, size_t fstride,
+                                                    const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int P = N + 1, NE = N * N;
+    static_assert(NE <= NT * E, "plane does not fit the thread block");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + N * P;
+    const int x = blockIdx.x;
+    const int f = blockIdx.y;
+    const size_t base = (size_t)f * fstride + (size_t)x * NE;
+    if (S1 != 0 || S2 != 0)
+        for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    if (S1 != 0) {
+        constexpr int U = 4;
+        for (int e0 = threadIdx.x; e0 < NE; e0 += U * NT) {
+            V v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (NE % (U * NT) == 0 || e < NE) v[u] = src[base + e];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (NE % (U * NT) == 0 || e < NE) tile[(e / N) * P + e % N] = v[u];
+            }
+        }
+        __syncthreads();
+        ct_fft<V, S1, N, RMAX, N, 1, P, NT, E>(tile, stw);   // z-lines
+        ct_fft<V, S1, N, RMAX, N, P, 1, NT, E>(tile, stw);   // y-lines
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < NE; e += NT) {
+        const int y = e / N, z = e % N;
+        V v = S1 != 0 ? tile[y * P + z] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z, base + e, v);
+        if (S2 != 0) tile[y * P + z] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        ct_fft<V, S2, N, RMAX, N, 1, P, NT, E>(tile, stw);
+        ct_fft<V, S2, N, RMAX, N, P, 1, NT, E>(tile, stw);
+        for (int e = threadIdx.x; e < NE; e += NT) dst[base + e] = tile[(e / N) * P + e % N];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// Strided pass: lines of length N along y (DIM 1, outer index x) or x (DIM 0,
+// outer index y), W contiguous z-columns per tile; grid (outer * M3/W, nf).
+template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx<T>* src, cplx<T>* dst,
+                                                      size_t fstride, const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int NE = N * W;
+    static_assert(NE <= NT * E, "tile does not fit the thread block");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + NE;
+    const int nzb = m3 / W;
+    const int outer = blockIdx.x / nzb;
+    const int z0 = (blockIdx.x - outer * nzb) * W;
+    const int f = blockIdx.y;
+    const size_t plane = (size_t)m2 * m3;
+    const size_t lstride = DIM == 1 ? (size_t)m3 : plane;
+    const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
+    if (S1 != 0 || S2 != 0)
+        for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    if (S1 != 0) {
+        constexpr int U = 4;
+        for (int e0 = threadIdx.x; e0 < NE; e0 += U * NT) {
+            V v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (NE % (U * NT) == 0 || e < NE) v[u] = src[base + (e / W) * lstride + e % W];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (NE % (U * NT) == 0 || e < NE) tile[e] = v[u];
+            }
+        }
+        __syncthreads();
+        ct_fft<V, S1, N, RMAX, W, W, 1, NT, E>(tile, stw);
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < NE; e += NT) {
+        const int j = e / W, w = e % W;
+        const int x = DIM == 1 ? outer : j;
+        const int y = DIM == 1 ? j : outer;
+        const size_t off = base + j * lstride + w;
+        V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z0 + w, off, v);
+        if (S2 != 0) tile[e] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        ct_fft<V, S2, N, RMAX, W, W, 1, NT, E>(tile, stw);
+        for (int e = threadIdx.x; e < NE; e += NT) dst[base + (e / W) * lstride + e % W] = tile[e];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// z-line pass: BR rows of length N per CTA; grid (m1*m2/BR, nf).
+template <typename T, int N, int BR, int RMAX, int NT, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, cplx<T>* dst, size_t fstride,
+                                                    const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int P = N + 1, NE = BR * N;
+    static_assert(NE <= NT * E, "tile does not fit the thread block");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + BR * P;
+    const int f = blockIdx.y;
+    const int row0 = blockIdx.x * BR;
+    const size_t base = (size_t)f * fstride + (size_t)row0 * N;
+    if (S1 != 0 || S2 != 0)
+        for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    if (S1 != 0) {
+        for (int e = threadIdx.x; e < NE; e += NT) tile[(e / N) * P + e % N] = src[base + e];
+        __syncthreads();
+        ct_fft<V, S1, N, RMAX, BR, 1, P, NT, E>(tile, stw);
+    } else {
+        __syncthreads();
+    }
+    op.begin();
+    for (int e = threadIdx.x; e < NE; e += NT) {
+        const int b = e / N, z = e % N;
+        const int row = row0 + b;
+        const int x = row / m2, y = row - x * m2;
+        V v = S1 != 0 ? tile[b * P + z] : mkc<V>(T(0), T(0));
+        v = op(f, x, y, z, base + e, v);
+        if (S2 != 0) tile[b * P + z] = v;
+    }
+    if (S2 != 0) {
+        __syncthreads();
+        ct_fft<V, S2, N, RMAX, BR, 1, P, NT, E>(tile, stw);
+        for (int e = threadIdx.x; e < NE; e += NT) dst[base + e] = tile[(e / N) * P + e % N];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
 
 }  // namespace ftsp

@@ -57,6 +57,10 @@ class ftsp_views(C.Structure):
                                           "dpsi_bar")]
 
 
+class ftsp_kernel_stat(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("launches", C.c_longlong), ("bytes", C.c_double)]
+
+
 _lib = None
 
 
@@ -92,6 +96,8 @@ def lib():
         L.ftsp_state_views.argtypes = [vp, C.POINTER(ftsp_views)]
         L.ftsp_last_launch_count.restype = C.c_longlong
         L.ftsp_last_launch_count.argtypes = [vp]
+        L.ftsp_profile_enable.argtypes = [vp, C.c_int]
+        L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -100,7 +106,7 @@ def lib():
 ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_stream", "ftsp_set_fields",
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
-               "ftsp_state_views", "ftsp_last_launch_count")
+               "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read")
 
 
 def _dp(a):
@@ -239,6 +245,21 @@ class Engine:
         rec = np.zeros(self.record_len, dtype=np.complex128)
         self._check(lib().ftsp_measure(self.h, which, rec.ctypes.data), "measure")
         return rec
+
+    def set_fields_ptr(self, omega_ptr: int, psi_ptr: int):
+        """set_fields from raw host pointers (e.g. pinned buffers)."""
+        self._check(lib().ftsp_set_fields(self.h, C.c_void_p(omega_ptr), C.c_void_p(psi_ptr)), "set_fields")
+
+    def profile(self, on: bool = True):
+        self._check(lib().ftsp_profile_enable(self.h, int(on)), "profile_enable")
+
+    def profile_read(self) -> dict:
+        n = C.c_int(0)
+        self._check(lib().ftsp_profile_read(self.h, None, 0, C.byref(n)), "profile_read")
+        buf = (ftsp_kernel_stat * max(1, n.value))()
+        self._check(lib().ftsp_profile_read(self.h, buf, n.value, C.byref(n)), "profile_read")
+        return {buf[i].name.decode(): {"ms": buf[i].ms, "launches": buf[i].launches, "bytes": buf[i].bytes}
+                for i in range(n.value)}
 
     def set_noise(self, eta):
         e = np.ascontiguousarray(np.asarray(eta, dtype=np.float64).reshape(-1))

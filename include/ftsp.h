@@ -160,6 +160,22 @@ int ftsp_state_views(ftsp_handle* h, ftsp_views* views);
  * ftsp_step_async. */
 long long ftsp_last_launch_count(const ftsp_handle* h);
 
+/* CUDA-event timing of the chain-propagator passes (no reference
+ * counterpart: the reference prints only its total wall time, main.cu:89-91).
+ * ftsp_profile_enable clears the accumulators; while enabled, every
+ * real-space segment pass and k-space bond pass is bracketed by events on the
+ * handle's stream.  ftsp_profile_read synchronises the stream and returns,
+ * per pass kind, the summed device time, the launch count and the
+ * algorithmic bytes (the minimum HBM traffic of the pass's work). */
+typedef struct ftsp_kernel_stat {
+    char name[48];
+    double ms;
+    long long launches;
+    double bytes;
+} ftsp_kernel_stat;
+int ftsp_profile_enable(ftsp_handle* h, int on);
+int ftsp_profile_read(ftsp_handle* h, ftsp_kernel_stat* out, int max_entries, int* count);
+
 #ifdef __cplusplus
 }
 #endif
