@@ -317,15 +317,23 @@ template <typename T>
 struct OpLoadN {
     const cplx<T>* s[16];
     size_t fs;
+    struct Pre {
+        cplx<T> v;
+    };
     __device__ __forceinline__ void begin() {}
-    __device__ __forceinline__ cplx<T> operator()(int f, int, int, int, size_t g, cplx<T>) const { return s[f][g - f * fs]; }
+    __device__ __forceinline__ Pre load(int f, size_t g) const { return Pre{s[f][g - f * fs]}; }
+    __device__ __forceinline__ cplx<T> apply(int, int, int, int, size_t, cplx<T>, const Pre& p) const { return p.v; }
     __device__ __forceinline__ void end(double*, size_t) {}
 };
 template <typename T>
 struct OpLoadOne {
     const cplx<T>* s;
+    struct Pre {
+        cplx<T> v;
+    };
     __device__ __forceinline__ void begin() {}
-    __device__ __forceinline__ cplx<T> operator()(int, int, int, int, size_t g, cplx<T>) const { return s[g]; }
+    __device__ __forceinline__ Pre load(int, size_t g) const { return Pre{s[g]}; }
+    __device__ __forceinline__ cplx<T> apply(int, int, int, int, size_t, cplx<T>, const Pre& p) const { return p.v; }
     __device__ __forceinline__ void end(double*, size_t) {}
 };
 

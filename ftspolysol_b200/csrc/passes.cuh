@@ -114,11 +114,24 @@ __global__ void __launch_bounds__(1024, 1) k_plane(PlaneGeom g, const cplx<T>* s
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int y = fdiv(e, g.fm3), z = e - y * g.m3;
-        V v = S1 != 0 ? tile[y * g.P + z] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z, base + e, v);
-        if (S2 != 0) tile[y * g.P + z] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    for (int e0 = threadIdx.x; e0 < ne; e0 += PB * blockDim.x) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) pre[k] = op.load(f, base + e);
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) {
+                const int y = fdiv(e, g.fm3), z = e - y * g.m3;
+                V v = S1 != 0 ? tile[y * g.P + z] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z, base + e, v, pre[k]);
+                if (S2 != 0) tile[y * g.P + z] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
@@ -160,13 +173,26 @@ __global__ void __launch_bounds__(256, 2) k_zline(LineGeom g, const cplx<T>* src
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int b = fdiv(e, g.fm3), z = e - b * g.m3;
-        const int row = row0 + b;
-        const int x = fdiv(row, g.fm2), y = row - x * g.m2;
-        V v = S1 != 0 ? tile[b * g.P + z] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z, base + e, v);
-        if (S2 != 0) tile[b * g.P + z] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    for (int e0 = threadIdx.x; e0 < ne; e0 += PB * blockDim.x) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) pre[k] = op.load(f, base + e);
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) {
+                const int b = fdiv(e, g.fm3), z = e - b * g.m3;
+                const int row = row0 + b;
+                const int x = fdiv(row, g.fm2), y = row - x * g.m2;
+                V v = S1 != 0 ? tile[b * g.P + z] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z, base + e, v, pre[k]);
+                if (S2 != 0) tile[b * g.P + z] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
@@ -223,14 +249,30 @@ __global__ void __launch_bounds__(256, 2) k_strided(LineGeom g, const cplx<T>* s
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        const int j = fdiv(e, g.fW), w = e - j * g.W;
-        const int x = DIM == 1 ? outer : j;
-        const int y = DIM == 1 ? j : outer;
-        const size_t off = base + j * lstride + w;
-        V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z0 + w, off, v);
-        if (S2 != 0) tile[e] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    for (int e0 = threadIdx.x; e0 < ne; e0 += PB * blockDim.x) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) {
+                const int j = fdiv(e, g.fW), w = e - j * g.W;
+                pre[k] = op.load(f, base + j * lstride + w);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = e0 + k * blockDim.x;
+            if (e < ne) {
+                const int j = fdiv(e, g.fW), w = e - j * g.W;
+                const int x = DIM == 1 ? outer : j;
+                const int y = DIM == 1 ? j : outer;
+                const size_t off = base + j * lstride + w;
+                V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z0 + w, off, v, pre[k]);
+                if (S2 != 0) tile[e] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
@@ -246,10 +288,17 @@ __global__ void __launch_bounds__(256, 2) k_strided(LineGeom g, const cplx<T>* s
 // ---------------------------------------------------------------------------
 // Pointwise ops
 // ---------------------------------------------------------------------------
+// Op interface: begin() once per thread; load(f, g) issues the global loads
+// an element needs and returns them (the kernels batch PB elements so that
+// many loads are in flight); apply(f, x, y, z, g, v, pre) does the element's
+// arithmetic and stores and returns the value for the second transform;
+// end(scratch, cta) closes per-block reductions.
 template <typename T>
 struct OpIdentity {
+    struct Pre {};
     __device__ __forceinline__ void begin() {}
-    __device__ __forceinline__ cplx<T> operator()(int, int, int, int, size_t, cplx<T> v) const { return v; }
+    __device__ __forceinline__ Pre load(int, size_t) const { return Pre{}; }
+    __device__ __forceinline__ cplx<T> apply(int, int, int, int, size_t, cplx<T> v, const Pre&) const { return v; }
     __device__ __forceinline__ void end(double*, size_t) {}
 };
 
@@ -277,20 +326,37 @@ struct OpProp {
     double acc[2];
     T fr, fi;
 
+    static constexpr bool FWD = KIND <= FWD_SINGLE;
+    static constexpr bool NEED_E = KIND == FWD_START || KIND == FWD_MID || KIND == FWD_LAST || KIND == FWD_SINGLE ||
+                                   KIND == BWD_START || KIND == BWD_MID;
+    struct Pre {
+        V e, q, r, c;
+    };
+
     __device__ __forceinline__ void begin()
     {
         acc[0] = acc[1] = 0.0;
-        if (KIND >= BWD_START) {
+        if (!FWD) {
             const double2 fc = *factor;
             fr = T(fc.x);
             fi = T(fc.y);
         }
     }
-    __device__ __forceinline__ V operator()(int, int, int, int, size_t g, V u)
+    __device__ __forceinline__ Pre load(int, size_t g) const
     {
-        if (KIND <= FWD_SINGLE) {
-            const V e = E[g];
-            const V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? e : cmul(u, e);
+        Pre p;
+        if (NEED_E) p.e = E[g];
+        if (!FWD) {
+            p.q = qread[g];
+            p.r = rho_type[g];
+            if (rho_charge) p.c = rho_charge[g];
+        }
+        return p;
+    }
+    __device__ __forceinline__ V apply(int, int, int, int, size_t g, V u, const Pre& p)
+    {
+        if (FWD) {
+            const V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? p.e : cmul(u, p.e);
             qstore[g] = q;
             if (KIND == FWD_LAST || KIND == FWD_SINGLE) {
                 acc[0] += (double)q.x;
@@ -298,17 +364,12 @@ struct OpProp {
             }
             return q;
         } else {
-            const V qf = qread[g];
-            const V phi = (KIND == BWD_START || KIND == BWD_SINGLE) ? qf : cmul(qf, u);
+            const V phi = (KIND == BWD_START || KIND == BWD_SINGLE) ? p.q : cmul(p.q, u);
             const V w = cmul(phi, mkc<V>(fr, fi));
-            V r = rho_type[g];
-            rho_type[g] = cadd(r, w);
-            if (rho_charge) {
-                V c = rho_charge[g];
-                rho_charge[g] = cadd(c, cscale(w, z));
-            }
-            if (KIND == BWD_START) return E[g];
-            if (KIND == BWD_MID) return cmul(u, E[g]);
+            rho_type[g] = cadd(p.r, w);
+            if (rho_charge) rho_charge[g] = cadd(p.c, cscale(w, z));
+            if (KIND == BWD_START) return p.e;
+            if (KIND == BWD_MID) return cmul(u, p.e);
             return u;
         }
     }
@@ -346,6 +407,9 @@ struct OpBond {
     const double2* factor;
     double2* partial;        // [cta][6] accumulated across bonds
     double acc[12];
+    struct Pre {
+        V F;
+    };
 
     __device__ __forceinline__ void begin()
     {
@@ -354,13 +418,19 @@ struct OpBond {
             for (int c = 0; c < 12; ++c) acc[c] = 0.0;
         }
     }
-    __device__ __forceinline__ V operator()(int, int x, int y, int z, size_t g, V v)
+    __device__ __forceinline__ Pre load(int, size_t g) const
+    {
+        Pre p;
+        if (!FWD && STRESS) p.F = Fread[g];
+        return p;
+    }
+    __device__ __forceinline__ V apply(int, int x, int y, int z, size_t g, V v, const Pre& pre)
     {
         const T phi = phix[x] * phiy[y] * phiz[z];
         if (FWD) {
             if (Fstore) Fstore[g] = v;
         } else if (STRESS) {
-            const V F = Fread[g];
+            const V F = pre.F;
             const V p = cmul(F, v);
             const double pr = (double)p.x * (double)phi, pi = (double)p.y * (double)phi;
             const double ax = kx[x], ay = ky[y], az = kz[z];
@@ -419,20 +489,18 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     if (S1 != 0 || S2 != 0)
         for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    constexpr int EPT = (NE + NT - 1) / NT;   // elements per thread
     if (S1 != 0) {
-        constexpr int U = 4;
-        for (int e0 = threadIdx.x; e0 < NE; e0 += U * NT) {
-            V v[U];
+        V v[EPT];   // every load of the thread in flight before the first smem store
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = e0 + u * NT;
-                if (NE % (U * NT) == 0 || e < NE) v[u] = src[base + e];
-            }
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) v[u] = src[base + e];
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = e0 + u * NT;
-                if (NE % (U * NT) == 0 || e < NE) tile[(e / N) * P + e % N] = v[u];
-            }
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) tile[(e / N) * P + e % N] = v[u];
         }
         __syncthreads();
         ct_fft<V, S1, N, RMAX, N, 1, P, NT, E>(tile, stw);   // z-lines
@@ -441,11 +509,25 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < NE; e += NT) {
-        const int y = e / N, z = e % N;
-        V v = S1 != 0 ? tile[y * P + z] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z, base + e, v);
-        if (S2 != 0) tile[y * P + z] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+#pragma unroll 1
+    for (int u0 = 0; u0 < EPT; u0 += PB) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) pre[k] = op.load(f, base + e);
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) {
+                const int y = e / N, z = e % N;
+                V v = S1 != 0 ? tile[y * P + z] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z, base + e, v, pre[k]);
+                if (S2 != 0) tile[y * P + z] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
@@ -477,20 +559,18 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
     const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
     if (S1 != 0 || S2 != 0)
         for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    constexpr int EPT = (NE + NT - 1) / NT;
     if (S1 != 0) {
-        constexpr int U = 4;
-        for (int e0 = threadIdx.x; e0 < NE; e0 += U * NT) {
-            V v[U];
+        V v[EPT];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = e0 + u * NT;
-                if (NE % (U * NT) == 0 || e < NE) v[u] = src[base + (e / W) * lstride + e % W];
-            }
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) v[u] = src[base + (e / W) * lstride + e % W];
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = e0 + u * NT;
-                if (NE % (U * NT) == 0 || e < NE) tile[e] = v[u];
-            }
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) tile[e] = v[u];
         }
         __syncthreads();
         ct_fft<V, S1, N, RMAX, W, W, 1, NT, E>(tile, stw);
@@ -498,14 +578,28 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < NE; e += NT) {
-        const int j = e / W, w = e % W;
-        const int x = DIM == 1 ? outer : j;
-        const int y = DIM == 1 ? j : outer;
-        const size_t off = base + j * lstride + w;
-        V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z0 + w, off, v);
-        if (S2 != 0) tile[e] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+#pragma unroll 1
+    for (int u0 = 0; u0 < EPT; u0 += PB) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) pre[k] = op.load(f, base + (e / W) * lstride + e % W);
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) {
+                const int j = e / W, w = e % W;
+                const int x = DIM == 1 ? outer : j;
+                const int y = DIM == 1 ? j : outer;
+                const size_t off = base + j * lstride + w;
+                V v = S1 != 0 ? tile[e] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z0 + w, off, v, pre[k]);
+                if (S2 != 0) tile[e] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
@@ -531,21 +625,46 @@ __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, 
     const size_t base = (size_t)f * fstride + (size_t)row0 * N;
     if (S1 != 0 || S2 != 0)
         for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    constexpr int EPT = (NE + NT - 1) / NT;
     if (S1 != 0) {
-        for (int e = threadIdx.x; e < NE; e += NT) tile[(e / N) * P + e % N] = src[base + e];
+        V v[EPT];
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) v[u] = src[base + e];
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = threadIdx.x + u * NT;
+            if (NE % NT == 0 || e < NE) tile[(e / N) * P + e % N] = v[u];
+        }
         __syncthreads();
         ct_fft<V, S1, N, RMAX, BR, 1, P, NT, E>(tile, stw);
     } else {
         __syncthreads();
     }
     op.begin();
-    for (int e = threadIdx.x; e < NE; e += NT) {
-        const int b = e / N, z = e % N;
-        const int row = row0 + b;
-        const int x = row / m2, y = row - x * m2;
-        V v = S1 != 0 ? tile[b * P + z] : mkc<V>(T(0), T(0));
-        v = op(f, x, y, z, base + e, v);
-        if (S2 != 0) tile[b * P + z] = v;
+    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+#pragma unroll 1
+    for (int u0 = 0; u0 < EPT; u0 += PB) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) pre[k] = op.load(f, base + e);
+        }
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+            const int e = threadIdx.x + (u0 + k) * NT;
+            if (u0 + k < EPT && (NE % NT == 0 || e < NE)) {
+                const int b = e / N, z = e % N;
+                const int row = row0 + b;
+                const int x = row / m2, y = row - x * m2;
+                V v = S1 != 0 ? tile[b * P + z] : mkc<V>(T(0), T(0));
+                v = op.apply(f, x, y, z, base + e, v, pre[k]);
+                if (S2 != 0) tile[b * P + z] = v;
+            }
+        }
     }
     if (S2 != 0) {
         __syncthreads();
