@@ -223,6 +223,15 @@ int ftsp_state_views(ftsp_handle* h, ftsp_views* v)
     return FTSP_OK;
 }
 
+int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_length, double* q_end, double* Q)
+{
+    if (!w || !q_end) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->propagate_chain(reinterpret_cast<const double2*>(w), N, bond_length,
+                                          reinterpret_cast<double2*>(q_end), Q));
+    if (Q && !(std::isfinite(Q[0]) && std::isfinite(Q[1]))) return FTSP_NONFINITE;
+    return FTSP_OK;
+}
+
 int ftsp_profile_enable(ftsp_handle* h, int on)
 {
     FTSP_GUARD(h, {

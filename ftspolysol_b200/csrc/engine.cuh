@@ -30,7 +30,7 @@ constexpr int MAXSP = 16;
 constexpr int MAXION = 16;
 constexpr int MAXM = 8;
 constexpr int MAXMODE = 8;
-constexpr int RED_BLOCKS = 296;   // fixed reduction grid (2 x 148 SMs) => deterministic sums
+constexpr int RED_BLOCKS = 1184;  // fixed reduction grid (8 x 148 SMs) => deterministic sums
 constexpr int RED_THREADS = 256;
 constexpr double PI = 3.141592653589793238462643383279502884;
 
@@ -58,6 +58,7 @@ struct DevScal {
     alignas(16) double corr[4];            // corrector: sum of psi (complex), non-finite cell count
     alignas(16) double fsq[2 * MAXMODE];   // sum over the grid of omega_a^2 (complex)
     alignas(16) double kobs[26];           // k-space observable sums
+    alignas(16) double sconn[12];          // connectivity stress sums over the bond-pass CTAs
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
     alignas(16) int nonfinite;
@@ -189,18 +190,23 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
     }
 }
 
-// Fixed-order combine of `count` partial rows of K channels.
+// Fixed-order combine of `count` partial rows of K channels: one warp per
+// channel (grid K), lanes stride over the rows, then a shuffle tree.
 template <bool MAX>
 __global__ void k_combine(const double* partial, int count, int K, double* out)
 {
-    for (int c = threadIdx.x; c < K; c += blockDim.x) {
-        double s = 0.0;
-        for (int b = 0; b < count; ++b) {
-            const double y = partial[(size_t)b * K + c];
-            s = MAX ? fmax(s, y) : s + y;
-        }
-        out[c] = s;
+    const int c = blockIdx.x;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < count; b += 32) {
+        const double y = partial[(size_t)b * K + c];
+        s = MAX ? fmax(s, y) : s + y;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, s, o);
+        s = MAX ? fmax(s, y) : s + y;
+    }
+    if (threadIdx.x == 0) out[c] = s;
 }
 
 // ---- small complex helpers in double ----
@@ -434,6 +440,7 @@ struct EngineBase {
     virtual int step(double* Qbar, double* rec, double* dmax, bool sync) = 0;
     virtual int read_status(double* rec, double* dmax) = 0;
     virtual void views(ftsp_views* v) = 0;
+    virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
 };
 
 template <typename T>
@@ -465,7 +472,7 @@ struct Engine : EngineBase {
     static constexpr int EP = F32 ? 32 : 16;   // elements per thread, runtime-plan plane pass
     static constexpr int EL = F32 ? 16 : 8;    // elements per thread, runtime-plan line passes
     static constexpr int RMAX = F32 ? 16 : 8;  // largest radix of the compile-time transforms
-    static constexpr int WCT = F32 ? 32 : 16;  // z-columns per tile of the compile-time strided passes
+    static constexpr int WCT = F32 ? 16 : 8;   // z-columns per tile of the compile-time strided passes (128-byte rows)
     Buf<FftPlan1> plans;                       // device-memory plans: x, y, z
 
     // device buffers
@@ -664,7 +671,7 @@ struct Engine : EngineBase {
     void reduce(size_t n, F f, double* out)
     {
         k_reduce<K, MAX><<<RED_BLOCKS, RED_THREADS, 0, stream>>>(n, f, part.p);
-        k_combine<MAX><<<1, 64, 0, stream>>>(part.p, RED_BLOCKS, K, out);
+        k_combine<MAX><<<K, 32, 0, stream>>>(part.p, RED_BLOCKS, K, out);
         launches += 2;
     }
 
@@ -886,17 +893,13 @@ struct Engine : EngineBase {
             const double nv = s.nc / c.volume;
             const double invV = 1.0 / (double)Vn;
             DevScal* d = ds;
+            k_combine<false><<<2, 32, 0, stream>>>(qpart, cnt, 2, reinterpret_cast<double*>(&d->Q[isp]));
             k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
-                double sx = 0.0, sy = 0.0;
-                for (int i = 0; i < cnt; ++i) {
-                    sx += qpart[2 * i];
-                    sy += qpart[2 * i + 1];
-                }
-                const double2 Q = make_double2(sx * invV, sy * invV);
+                const double2 Q = dscale(d->Q[isp], invV);
                 d->Q[isp] = Q;
                 d->factor[isp] = dscale(dinv(Q), nv);
             });
-            ++launches;
+            launches += 2;
         }
         // ---- backward sweep (opposite sign convention: B' = B(-k)) ----
         auto rho_of = [&](int seg) { return dB.p + (size_t)s.type[seg] * Vn; };
@@ -1380,6 +1383,10 @@ struct Engine : EngineBase {
 
     void finalize_record(bool with_stress)
     {
+        if (with_stress) {
+            k_combine<false><<<12, 32, 0, stream>>>(spart.p, x_ctas(), 12, ds->sconn);
+            ++launches;
+        }
         const int S = (int)c.sp.size(), J = (int)c.ions.size(), nm = c.nm;
         RecConst rc{};
         for (int s = 0; s < S; ++s) {
@@ -1433,8 +1440,6 @@ struct Engine : EngineBase {
         const double invV = 1.0 / (double)V_;
         const double lB = c.lB;
         const bool elec = c.elec;
-        const int nx = x_ctas();
-        const double* sp = spart.p;
         DevScal* d = ds;
         const bool ws = with_stress;
         k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
@@ -1459,14 +1464,7 @@ struct Engine : EngineBase {
             if (ws) {
                 // connectivity sums over the bond-pass CTAs
                 double2 Sc[6];
-                for (int cc = 0; cc < 6; ++cc) {
-                    double sx = 0.0, sy = 0.0;
-                    for (int b = 0; b < nx; ++b) {
-                        sx += sp[(size_t)b * 12 + 2 * cc];
-                        sy += sp[(size_t)b * 12 + 2 * cc + 1];
-                    }
-                    Sc[cc] = make_double2(sx, sy);
-                }
+                for (int cc = 0; cc < 6; ++cc) Sc[cc] = make_double2(d->sconn[2 * cc], d->sconn[2 * cc + 1]);
                 const double2 V0 = make_double2(ko[12], ko[13]);
                 for (int q = 0; q < na; ++q) {
                     const int cc = rc.active[q];
@@ -1678,6 +1676,81 @@ struct Engine : EngineBase {
     }
 
     int read_status(double* rec, double* dmax) override { return read_status_impl(nullptr, rec, dmax); }
+
+    // Forward propagators of N identical segments in the field w (device,
+    // complex128): q_1 = exp(-w), q_{s+1} = exp(-w) IFFT[Phi FFT[q_s] / V],
+    // Phi = exp(-b^2 k^2 / 6); q_N to q_end (device), Q = mean(q_N) to the
+    // host.  Uses the handle's class-table slot 0, G and the reduction
+    // partials as scratch.
+    Buf<T> phi_user;
+    double phi_user_b = -1.0;
+
+    void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Qh) override
+    {
+        if (sizeof(T) != 8) throw std::runtime_error("ftsp_propagate_chain needs a complex128 (FP64) handle");
+        if (N < 1) throw std::runtime_error("ftsp_propagate_chain: N must be >= 1");
+        if (!(bond > 0.0)) throw std::runtime_error("ftsp_propagate_chain: bond length must be positive");
+        const size_t Vn = V_;
+        V* Ep = E.p;
+        const V* wp = reinterpret_cast<const V*>(w);
+        foreach(Vn, [=] __device__(size_t i) {
+            const V x = wp[i];
+            Ep[i] = cexpT(-x.x, -x.y);
+        });
+        const int sum_m = c.m1 + c.m2 + c.m3;
+        if (!phi_user.p) phi_user.alloc(sum_m);
+        if (phi_user_b != bond) {
+            std::vector<T> t;
+            for (int i = 0; i < c.m1; ++i) { const double k = wave_number(i, c.m1, c.L[0]); t.push_back((T)std::exp(-bond * bond * k * k / 6.0)); }
+            for (int i = 0; i < c.m2; ++i) { const double k = wave_number(i, c.m2, c.L[1]); t.push_back((T)std::exp(-bond * bond * k * k / 6.0)); }
+            for (int i = 0; i < c.m3; ++i) { const double k = wave_number(i, c.m3, c.L[2]); t.push_back((T)std::exp(-bond * bond * k * k / 6.0)); }
+            FTSP_CUDA(cudaMemcpyAsync(phi_user.p, t.data(), sizeof(T) * t.size(), cudaMemcpyHostToDevice, stream));
+            FTSP_CUDA(cudaStreamSynchronize(stream));
+            phi_user_b = bond;
+        }
+        V* qe = reinterpret_cast<V*>(q_end);
+        double2* qpart = reinterpret_cast<double2*>(part.p);
+        auto bond_op = [&]() {
+            OpBond<T, true, false> ob{};
+            ob.phix = phi_user.p;
+            ob.phiy = phi_user.p + c.m1;
+            ob.phiz = phi_user.p + c.m1 + c.m2;
+            ob.kx = kx.p; ob.ky = ky.p; ob.kz = kz.p;
+            ob.invV = (T)(1.0 / (double)Vn);
+            return ob;
+        };
+        if (N == 1) {
+            OpProp<T, FWD_SINGLE> op{};
+            op.E = Ep; op.qstore = qe; op.partial = qpart;
+            seg_pass<0, 0, FWD_SINGLE>(nullptr, nullptr, op);
+        } else {
+            OpProp<T, FWD_START> op0{};
+            op0.E = Ep; op0.qstore = qe;
+            seg_pass<0, -1, FWD_START>(nullptr, G.p, op0);
+            for (int b = 0; b < N - 1; ++b) {
+                bond_pass<-1, +1, true, false>(G.p, G.p, bond_op());
+                if (b + 1 < N - 1) {
+                    OpProp<T, FWD_MID> op{};
+                    op.E = Ep; op.qstore = qe;
+                    seg_pass<+1, -1, FWD_MID>(G.p, G.p, op);
+                } else {
+                    OpProp<T, FWD_LAST> op{};
+                    op.E = Ep; op.qstore = qe; op.partial = qpart;
+                    seg_pass<+1, 0, FWD_LAST>(G.p, nullptr, op);
+                }
+            }
+        }
+        double* out = reinterpret_cast<double*>(&ds->Q[0]);
+        k_combine<false><<<2, 32, 0, stream>>>(part.p, seg_pass_ctas(), 2, out);
+        ++launches;
+        double q[2];
+        FTSP_CUDA(cudaMemcpyAsync(q, out, sizeof(q), cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        if (Qh) {
+            Qh[0] = q[0] / (double)Vn;
+            Qh[1] = q[1] / (double)Vn;
+        }
+    }
 
     void views(ftsp_views* v) override
     {

@@ -96,6 +96,7 @@ def lib():
         L.ftsp_state_views.argtypes = [vp, C.POINTER(ftsp_views)]
         L.ftsp_last_launch_count.restype = C.c_longlong
         L.ftsp_last_launch_count.argtypes = [vp]
+        L.ftsp_propagate_chain.argtypes = [vp, vp, C.c_int, C.c_double, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
         L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
         _lib = L
@@ -106,7 +107,8 @@ def lib():
 ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_stream", "ftsp_set_fields",
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
-               "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read")
+               "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
+               "ftsp_propagate_chain")
 
 
 def _dp(a):
@@ -249,6 +251,13 @@ class Engine:
     def set_fields_ptr(self, omega_ptr: int, psi_ptr: int):
         """set_fields from raw host pointers (e.g. pinned buffers)."""
         self._check(lib().ftsp_set_fields(self.h, C.c_void_p(omega_ptr), C.c_void_p(psi_ptr)), "set_fields")
+
+    def propagate_chain(self, w_ptr: int, N: int, bond_length: float, q_end_ptr: int) -> complex:
+        """Chain propagation in an external field (device pointers, complex128)."""
+        Q = np.zeros(2)
+        self._check(lib().ftsp_propagate_chain(self.h, C.c_void_p(w_ptr), int(N), float(bond_length),
+                                               C.c_void_p(q_end_ptr), Q.ctypes.data), "propagate_chain")
+        return complex(Q[0], Q[1])
 
     def profile(self, on: bool = True):
         self._check(lib().ftsp_profile_enable(self.h, int(on)), "profile_enable")

@@ -136,6 +136,15 @@ int ftsp_step(ftsp_handle* h, double* Q_bar, double* record, double* drift_max);
 int ftsp_step_async(ftsp_handle* h);
 int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max);
 
+/* Forward propagators of a chain of N identical segments in an external
+ * field: q_1 = exp(-w), q_{s+1} = exp(-w) IFFT[Phi FFT[q_s] / V] with
+ * Phi(k) = exp(-b^2 k^2 / 6); returns q_N in q_end and Q = mean(q_N) in
+ * Q[0..1] (host).  w and q_end are device arrays of V complex128 values on the
+ * handle's grid; complex128 handles only.  Replaces
+ * polymerSpecies::propagate_chain and the Q of solve_chain_species_prepared
+ * (polymer.cu:402-426) for one segment class.  Scratch: the handle's buffers. */
+int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_length, double* q_end, double* Q);
+
 /* Device pointers of the resident state (FP64 handles only), in the layout of
  * deviceState (deviceState.h:6-48). */
 typedef struct ftsp_views {
