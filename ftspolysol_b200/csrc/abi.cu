@@ -3,6 +3,8 @@
 // CUDA errors and turns them into status codes; nothing calls exit().
 #include "engine.cuh"
 
+#include <mutex>
+
 namespace ftsp {
 
 HostCfg make_cfg(const ftsp_config* in)
@@ -87,6 +89,11 @@ struct ftsp_handle {
 };
 
 static thread_local std::string g_create_error;
+
+namespace ftsp {
+// Error text of handle-less calls, read back with ftsp_last_error(NULL).
+void set_thread_error(const std::string& s) { g_create_error = s; }
+}  // namespace ftsp
 
 #define FTSP_GUARD(h, body)                                      \
     do {                                                         \
@@ -265,3 +272,235 @@ long long ftsp_last_launch_count(const ftsp_handle* h)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Chain propagation without any device allocation.
+//
+// For callers that cannot call cudaMalloc: code running while a CUDA stream
+// is being captured into a graph (allocation calls are not allowed there),
+// code inside a framework whose caching allocator owns the device memory
+// (e.g. a PyTorch process that has reserved the pool), and real-time loops
+// that must not block on the driver's allocator.  It computes exactly what
+// ftsp_propagate_chain computes, but all of its scratch lives in the single
+// file-scope array below, so no call allocates or frees device memory.
+//
+// Limits: at most NOALLOC_MAX_POINTS grid points (64^3) and NOALLOC_MAX_EXTENT
+// points along any axis; complex128 only.  The array (about 8.3 MiB) is part
+// of the library image, so every GPU that loads libftsp.so holds it until the
+// process exits.  Every call on a device shares it: calls whose work overlaps
+// on the GPU (different streams, or different host threads) race on it and
+// must be serialised by the caller.  Each call writes every part of the
+// scratch it later reads (the exp(-w) table, the intermediate field, the
+// reduction partials, the FFT and bond tables), so no region has to start at
+// zero and nothing carries over from the previous call.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t NOALLOC_MAX_POINTS = 262144;   // 64^3
+constexpr int NOALLOC_MAX_EXTENT = 256;
+constexpr size_t NA_FIELD = NOALLOC_MAX_POINTS * sizeof(double2);      // 4 MiB
+constexpr size_t NA_PARTIALS_N = 16384;
+constexpr size_t NA_PARTIALS = NA_PARTIALS_N * sizeof(double2);       // 256 KiB
+constexpr size_t NA_TABLES = 64 * 1024;
+constexpr size_t NA_BYTES = 2 * NA_FIELD + NA_PARTIALS + NA_TABLES;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+std::mutex g_noalloc_mutex;
+constexpr int NA_MAX_DEVICES = 128;
+unsigned char* g_noalloc_base[NA_MAX_DEVICES] = {};
+
+// Small tables copied into the scratch at every call.
+struct NoallocTables {
+    ftsp::FftPlan1 plans[3];                 // x, y, z
+    double2 tw[3][NOALLOC_MAX_EXTENT];       // exp(-2 pi i j / m_d)
+    double phi[3 * NOALLOC_MAX_EXTENT];      // separable exp(-b^2 k_d^2 / 6)
+    double qsum[2];                          // sum of q_N (combine output)
+};
+static_assert(sizeof(NoallocTables) <= NA_TABLES, "noalloc tables do not fit their region");
+
+}  // namespace
+
+namespace ftsp {
+void set_thread_error(const std::string& s);
+}
+
+extern "C" int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, double L3,
+                                            const double* w, int N, double bond_length, double* q_end, double* Q,
+                                            void* cuda_stream)
+{
+    using namespace ftsp;
+    try {
+        if (!w || !q_end || !Q) throw std::runtime_error("ftsp_propagate_chain_noalloc: null argument");
+        if (m1 < 1 || m2 < 1 || m3 < 1) throw std::runtime_error("ftsp_propagate_chain_noalloc: invalid mesh");
+        if (m1 > NOALLOC_MAX_EXTENT || m2 > NOALLOC_MAX_EXTENT || m3 > NOALLOC_MAX_EXTENT)
+            throw std::runtime_error("ftsp_propagate_chain_noalloc: an extent exceeds the limit of " +
+                                     std::to_string(NOALLOC_MAX_EXTENT));
+        const size_t V = (size_t)m1 * m2 * m3;
+        if (V > NOALLOC_MAX_POINTS)
+            throw std::runtime_error("ftsp_propagate_chain_noalloc: " + std::to_string(V) +
+                                     " grid points exceed the limit of " + std::to_string(NOALLOC_MAX_POINTS) +
+                                     " (64^3); use ftsp_propagate_chain for larger grids");
+        if (N < 1) throw std::runtime_error("ftsp_propagate_chain_noalloc: N must be >= 1");
+        if (!(bond_length > 0.0)) throw std::runtime_error("ftsp_propagate_chain_noalloc: bond length must be positive");
+        if (!(L1 > 0.0 && L2 > 0.0 && L3 > 0.0)) throw std::runtime_error("ftsp_propagate_chain_noalloc: box lengths must be positive");
+        cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+
+        // one-time set-up per device: the device address of the scratch array
+        int dev = 0;
+        FTSP_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= NA_MAX_DEVICES) throw std::runtime_error("ftsp_propagate_chain_noalloc: device ordinal out of range");
+        unsigned char* base = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+            if (!g_noalloc_base[dev]) {
+                void* ptr = nullptr;
+                const cudaError_t err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+                if (err != cudaSuccess)
+                    throw std::runtime_error(std::string("ftsp_propagate_chain_noalloc: cudaGetSymbolAddress failed: ") +
+                                             cudaGetErrorString(err));
+                g_noalloc_base[dev] = static_cast<unsigned char*>(ptr);
+            }
+            base = g_noalloc_base[dev];
+        }
+        double2* Eb = reinterpret_cast<double2*>(base);
+        double2* Gb = reinterpret_cast<double2*>(base + NA_FIELD);
+        double2* partials = reinterpret_cast<double2*>(base + 2 * NA_FIELD);
+        NoallocTables* dtab = reinterpret_cast<NoallocTables*>(base + 2 * NA_FIELD + NA_PARTIALS);
+
+        // host tables: plans, twiddles, bond factors
+        NoallocTables ht{};
+        const int ms[3] = {m1, m2, m3};
+        const double Ls[3] = {L1, L2, L3};
+        for (int d = 0; d < 3; ++d) {
+            ht.plans[d] = make_plan(ms[d]);
+            for (int j = 0; j < ms[d]; ++j) {
+                const long double ang = -2.0L * 3.141592653589793238462643383279502884L * j / ms[d];
+                ht.tw[d][j] = make_double2((double)cosl(ang), (double)sinl(ang));
+            }
+        }
+        int off = 0;
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < ms[d]; ++i) {
+                const double k = wave_number(i, ms[d], Ls[d]);
+                ht.phi[off++] = std::exp(-bond_length * bond_length * k * k / 6.0);
+            }
+        FTSP_CUDA(cudaMemcpyAsync(dtab, &ht, sizeof(ht), cudaMemcpyHostToDevice, stream));
+
+        // launch geometry of the runtime-plan passes (complex128)
+        int dev_smem = 0;
+        FTSP_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        constexpr int EP = 16, EL = 8;
+        auto round32 = [](int t) { return std::max(32, (t + 31) / 32 * 32); };
+        PlaneGeom pg{};
+        pg.m1 = m1; pg.m2 = m2; pg.m3 = m3; pg.P = m3 + 1;
+        pg.py = &dtab->plans[1];
+        pg.pz = &dtab->plans[2];
+        pg.fm2 = make_fastdiv(m2);
+        pg.fm3 = make_fastdiv(m3);
+        const size_t plane_smem = std::max(sizeof(double2) * ((size_t)m2 * pg.P + m2 + m3), (size_t)4096);
+        const int plane_threads = round32((m2 * m3 + EP - 1) / EP);
+        const bool plane_ok = plane_smem <= (size_t)dev_smem && plane_threads <= 512;
+        int W = 1;
+        const int wmax = std::max(1, std::min(16, (EL * 256) / std::max(m1, m2)));
+        for (int cand = 1; cand <= std::min(m3, wmax); ++cand)
+            if (m3 % cand == 0) W = cand;
+        LineGeom gx{m1, m2, m3, m1, W, 0, W, &dtab->plans[0], make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
+        LineGeom gy{m1, m2, m3, m2, W, 0, W, &dtab->plans[1], make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
+        int B = std::max(1, 2048 / m3);
+        while ((m1 * m2) % B) --B;
+        LineGeom gz{m1, m2, m3, m3, 0, B, m3 + 1, &dtab->plans[2], make_fastdiv(1), make_fastdiv(B), make_fastdiv(m2), make_fastdiv(m3)};
+        const int x_threads = round32((m1 * W + EL - 1) / EL);
+        const int y_threads = round32((m2 * W + EL - 1) / EL);
+        const int z_threads = round32((B * m3 + EL - 1) / EL);
+        const size_t x_smem = std::max(sizeof(double2) * ((size_t)m1 * W + m1), (size_t)4096);
+        const size_t y_smem = std::max(sizeof(double2) * ((size_t)m2 * W + m2), (size_t)4096);
+        const size_t z_smem = std::max(sizeof(double2) * ((size_t)B * (m3 + 1) + m3), (size_t)4096);
+        if (x_threads > 256 || y_threads > 256 || z_threads > 256) throw std::runtime_error("ftsp_propagate_chain_noalloc: mesh too large for the line passes");
+        const int parts = plane_ok ? m1 : m1 * m2 / B;
+        if ((size_t)parts > NA_PARTIALS_N) throw std::runtime_error("ftsp_propagate_chain_noalloc: too many reduction partials");
+        const double2* tw1 = dtab->tw[0];
+        const double2* tw2 = dtab->tw[1];
+        const double2* tw3 = dtab->tw[2];
+        auto smem_attr = [&](auto kernel, size_t bytes) {
+            if (bytes > 48 * 1024) FTSP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        };
+        // real-space pass of one segment (plane, or y / z-line / y)
+        auto seg = [&](auto s1c, auto s2c, const double2* src, double2* dst, const auto& op) {
+            constexpr int S1 = decltype(s1c)::value, S2 = decltype(s2c)::value;
+            using Op = std::decay_t<decltype(op)>;
+            if (plane_ok) {
+                auto k = k_plane<double, EP, S1, S2, Op>;
+                smem_attr(k, plane_smem);
+                k<<<dim3(m1, 1), plane_threads, plane_smem, stream>>>(pg, src, dst, V, tw2, tw3, op);
+                return;
+            }
+            if (S1 != 0) {
+                auto k = k_strided<double, EL, 1, 0, S1, OpLoadOne<double>>;
+                smem_attr(k, y_smem);
+                k<<<dim3(m1 * (m3 / W), 1), y_threads, y_smem, stream>>>(gy, nullptr, const_cast<double2*>(src), V, tw2, OpLoadOne<double>{src});
+            }
+            auto kz = k_zline<double, EL, S1, S2, Op>;
+            smem_attr(kz, z_smem);
+            kz<<<dim3(m1 * m2 / B, 1), z_threads, z_smem, stream>>>(gz, src, dst, V, tw3, op);
+            if (S2 != 0) {
+                auto k = k_strided<double, EL, 1, 0, S2, OpLoadOne<double>>;
+                smem_attr(k, y_smem);
+                k<<<dim3(m1 * (m3 / W), 1), y_threads, y_smem, stream>>>(gy, nullptr, dst, V, tw2, OpLoadOne<double>{dst});
+            }
+        };
+        OpBond<double, true, false> ob{};
+        ob.phix = dtab->phi;
+        ob.phiy = dtab->phi + m1;
+        ob.phiz = dtab->phi + m1 + m2;
+        ob.invV = 1.0 / (double)V;
+        auto kb = k_strided<double, EL, 0, -1, +1, OpBond<double, true, false>>;
+        smem_attr(kb, x_smem);
+
+        const double2* wp = reinterpret_cast<const double2*>(w);
+        double2* qe = reinterpret_cast<double2*>(q_end);
+        {
+            const int blocks = (int)std::min<size_t>((V + 255) / 256, 148 * 16);
+            k_foreach<<<std::max(1, blocks), 256, 0, stream>>>(V, [=] __device__(size_t i) {
+                const double2 x = wp[i];
+                Eb[i] = cexpT(-x.x, -x.y);
+            });
+        }
+        using I0 = std::integral_constant<int, 0>;
+        using Ip = std::integral_constant<int, +1>;
+        using Im = std::integral_constant<int, -1>;
+        if (N == 1) {
+            OpProp<double, FWD_SINGLE> op{};
+            op.E = Eb; op.qstore = qe; op.partial = partials;
+            seg(I0{}, I0{}, nullptr, nullptr, op);
+        } else {
+            OpProp<double, FWD_START> op0{};
+            op0.E = Eb; op0.qstore = qe;
+            seg(I0{}, Im{}, nullptr, Gb, op0);
+            for (int b = 0; b < N - 1; ++b) {
+                kb<<<dim3(m2 * (m3 / W), 1), x_threads, x_smem, stream>>>(gx, Gb, Gb, V, tw1, ob);
+                if (b + 1 < N - 1) {
+                    OpProp<double, FWD_MID> op{};
+                    op.E = Eb; op.qstore = qe;
+                    seg(Ip{}, Im{}, Gb, Gb, op);
+                } else {
+                    OpProp<double, FWD_LAST> op{};
+                    op.E = Eb; op.qstore = qe; op.partial = partials;
+                    seg(Ip{}, I0{}, Gb, nullptr, op);
+                }
+            }
+        }
+        k_combine<false><<<2, 32, 0, stream>>>(reinterpret_cast<const double*>(partials), parts, 2, dtab->qsum);
+        FTSP_CUDA(cudaGetLastError());
+        double qs[2] = {0.0, 0.0};
+        FTSP_CUDA(cudaMemcpyAsync(qs, dtab->qsum, sizeof(qs), cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        Q[0] = qs[0] / (double)V;
+        Q[1] = qs[1] / (double)V;
+        if (!(std::isfinite(Q[0]) && std::isfinite(Q[1]))) return FTSP_NONFINITE;
+        return FTSP_OK;
+    } catch (const std::exception& e) {
+        ftsp::set_thread_error(e.what());
+        return FTSP_ERROR;
+    }
+}

@@ -97,6 +97,8 @@ def lib():
         L.ftsp_last_launch_count.restype = C.c_longlong
         L.ftsp_last_launch_count.argtypes = [vp]
         L.ftsp_propagate_chain.argtypes = [vp, vp, C.c_int, C.c_double, vp, vp]
+        L.ftsp_propagate_chain_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                                   vp, C.c_int, C.c_double, vp, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
         L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
         _lib = L
@@ -108,7 +110,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
-               "ftsp_propagate_chain")
+               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc")
 
 
 def _dp(a):
@@ -117,6 +119,28 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def propagate_chain_noalloc(m, L, w_ptr: int, N: int, bond_length: float, q_end_ptr: int, stream: int = 0):
+    """Chain propagation that allocates no device memory (no handle needed).
+
+    For callers that cannot allocate: inside CUDA stream capture, under a
+    framework that owns the device memory pool, or in loops that must not
+    wait on the allocator.  w and q_end are device pointers to m1*m2*m3
+    complex128 values; at most 64^3 points and 256 per axis.  Make the first
+    call on a device before any stream capture (it looks up the scratch
+    address), and do not run calls concurrently: they share one scratch
+    array.  Returns (status, Q)."""
+    Q = np.zeros(2)
+    rc = lib().ftsp_propagate_chain_noalloc(int(m[0]), int(m[1]), int(m[2]), float(L[0]), float(L[1]), float(L[2]),
+                                            C.c_void_p(w_ptr), int(N), float(bond_length), C.c_void_p(q_end_ptr),
+                                            Q.ctypes.data, C.c_void_p(stream))
+    return rc, complex(Q[0], Q[1])
+
+
+def last_error() -> str:
+    """Error text of the last failed handle-less call on this thread."""
+    return (lib().ftsp_last_error(None) or b"").decode()
 
 
 class Engine:

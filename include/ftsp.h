@@ -145,6 +145,25 @@ int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max);
  * (polymer.cu:402-426) for one segment class.  Scratch: the handle's buffers. */
 int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_length, double* q_end, double* Q);
 
+/* ftsp_propagate_chain without any device allocation, for callers that
+ * cannot call cudaMalloc: code that runs while a stream is being captured
+ * into a CUDA graph, code inside a framework whose caching allocator owns the
+ * device memory, real-time loops that must not block on the allocator.  No
+ * counterpart in the reference.  No handle: the mesh (m1..m3) and box
+ * lengths (L1..L3) are passed directly; w and q_end are device arrays of
+ * m1*m2*m3 complex128 values, Q (host) receives mean(q_N).  All scratch lives
+ * in one static device array of about 8.3 MiB inside the library, which every
+ * GPU that loads libftsp.so keeps until the process exits.  Limits: at most
+ * 262144 grid points (64^3) and 256 points per axis; larger meshes return
+ * FTSP_ERROR with the reason in ftsp_last_error(NULL).  The first call on a
+ * device looks the scratch address up with cudaGetSymbolAddress, so make that
+ * first call before any stream capture begins.  Calls that overlap on the GPU
+ * share the one scratch array and race: serialise them.  Runs on cuda_stream
+ * (NULL: the legacy default stream) and returns after the stream has
+ * finished the call's work. */
+int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, double L3, const double* w, int N,
+                                 double bond_length, double* q_end, double* Q, void* cuda_stream);
+
 /* Device pointers of the resident state (FP64 handles only), in the layout of
  * deviceState (deviceState.h:6-48). */
 typedef struct ftsp_views {
