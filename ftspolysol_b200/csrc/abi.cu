@@ -74,6 +74,7 @@ HostCfg make_cfg(const ftsp_config* in)
     c.precision = in->precision;
     c.scheme = in->scheme;
     c.device = in->device;
+    c.restart_interval = in->restart_interval > 0 ? in->restart_interval : 0;
     if (c.record_len() > 128) throw std::runtime_error("observable record too long");
     return c;
 }
@@ -237,6 +238,17 @@ int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_len
                                           reinterpret_cast<double2*>(q_end), Q));
     if (Q && !(std::isfinite(Q[0]) && std::isfinite(Q[1]))) return FTSP_NONFINITE;
     return FTSP_OK;
+}
+
+long long ftsp_restart_count(ftsp_handle* h)
+{
+    if (!h || !h->eng) return -1;
+    try {
+        return h->eng->restarts();
+    } catch (const std::exception& e_) {
+        h->err = e_.what();
+        return -1;
+    }
 }
 
 int ftsp_profile_enable(ftsp_handle* h, int on)

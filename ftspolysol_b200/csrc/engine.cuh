@@ -62,6 +62,8 @@ struct DevScal {
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
     alignas(16) int nonfinite;
+    int bad_last;                          // the last step produced a non-finite value
+    int restarts;                          // checkpoint rollbacks so far
 };
 static_assert(offsetof(DevScal, rec) % 16 == 0 && offsetof(DevScal, corr) % 16 == 0, "DevScal alignment");
 
@@ -102,6 +104,7 @@ struct HostCfg {
     bool noise;
     uint64_t seed;
     int precision, scheme, device;
+    int restart_interval;   // device checkpoint every so many steps; rollback on a non-finite step (0: off)
     int n_stress() const { return __builtin_popcount(stress_mask); }
     bool stress_on() const { return stress_mask != 0 || iso; }
     int record_len() const
@@ -291,6 +294,9 @@ struct ModeTab {
 struct SigTab {
     double s[MAXMODE + 1];
 };
+struct SiOTab {
+    double O[MAXMODE * MAXM];
+};
 struct ClsTab {
     int type[64];
     double z[64];
@@ -441,6 +447,7 @@ struct EngineBase {
     virtual int read_status(double* rec, double* dmax) = 0;
     virtual void views(ftsp_views* v) = 0;
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
+    virtual long long restarts() = 0;
 };
 
 template <typename T>
@@ -491,6 +498,11 @@ struct Engine : EngineBase {
     Buf<V> E;            // class tables exp(-W_c)
     Buf<V> qF, Fst, G, H;
     Buf<double> part;    // reduction partials
+    Buf<int> expo;       // propagator renormalisation exponents: forward [Nmax], backward [Nmax]
+    Buf<T> si_P;         // semi-implicit preconditioner 1/(1 + lambda dt G(k)): modes, then psi
+    Buf<V> si_inc;       // semi-implicit increments (nm + 1 fields)
+    Buf<V> ck;           // device checkpoint of (omega, psi) for rollback
+    Buf<float> pmax;     // per-CTA propagator maxima, two slots (ping-pong by segment parity)
     Buf<double> spart;   // stress partials [ncta_x * 6] complex
     DevScal* ds = nullptr;
     DevScal hs{};
@@ -515,7 +527,8 @@ struct Engine : EngineBase {
         for (auto* b : vb) b->release();
         plans.release();
         kx.release(); ky.release(); kz.release(); phi.release(); gam.release(); gion.release(); eta.release();
-        part.release(); spart.release(); stage.release();
+        part.release(); spart.release(); stage.release(); expo.release(); pmax.release();
+        si_P.release(); si_inc.release(); ck.release();
         if (ds) cudaFree(ds);
         release_events();
     }
@@ -598,7 +611,10 @@ struct Engine : EngineBase {
         if (c.stress_on()) Fst.alloc(Vn * Nmax);
         G.alloc(Vn); H.alloc(Vn);
         part.alloc((size_t)std::max(RED_BLOCKS, std::max(c.m1, c.m1 * c.m2)) * 32);
+        expo.alloc((size_t)2 * Nmax);
+        pmax.alloc((size_t)2 * std::max(c.m1, c.m1 * c.m2));
         spart.alloc((size_t)c.m2 * c.m3 * 12);
+        if (c.restart_interval > 0) ck.alloc((size_t)(std::max(1, c.nm) + 1) * V_);
         FTSP_CUDA(cudaMalloc(&ds, sizeof(DevScal)));
         FTSP_CUDA(cudaMemset(ds, 0, sizeof(DevScal)));
         FTSP_CUDA(cudaMemset(omega.p, 0, sizeof(V) * nmv));
@@ -654,6 +670,139 @@ struct Engine : EngineBase {
         }
         if (gi.empty()) gi = sep(0.0);
         upload(gion, gi);
+        if (c.scheme == FTSP_SCHEME_SI) build_si_tables();
+    }
+
+    // ---- semi-implicit preconditioner (no reference counterpart) ----
+    // Linear response of the drifts at the homogeneous state, per k:
+    //   G_a(k)   = c_a - Re(gamma_a^2) Gamma(k)^2 sum_sp (n_sp/V) S_oo(k),  o_s = O_{a, type(s)}
+    //   G_psi(k) = k^2/(4 pi lB) + Gamma(k)^2 sum_sp (n_sp/V) S_zz(k) + sum_j (n_j/V) z_j^2 Gamma_j(k)^2
+    // with the discrete-Gaussian-chain correlation sum
+    //   S_ww(k) = sum_{s,s'} w_s w_s' prod_{t between s and s'} exp(-b_t^2 k^2/6),
+    // evaluated by the recursion F_s = phi_{s-1} F_{s-1} + w_s,
+    // S += w_s (w_s + 2 phi_{s-1} F_{s-1}).  The chain terms vanish at k = 0
+    // (the densities are normalised by Q).  G_a is clipped at zero.  The
+    // update divides each increment by P^-1 = 1 + lambda dt G(k).
+    void build_si_tables()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        si_P.alloc((size_t)(nm + 1) * Vn);
+        si_inc.alloc((size_t)(nm + 1) * Vn);
+        // segment data: per segment (type, charge, bond class of the bond to the next segment)
+        std::vector<int> stype, sbond, soff, sN;
+        std::vector<double> schg, snv;
+        for (auto& s : c.sp) {
+            soff.push_back((int)stype.size());
+            sN.push_back(s.N);
+            snv.push_back(s.nc / c.volume);
+            for (int t = 0; t < s.N; ++t) {
+                stype.push_back(s.type[t]);
+                schg.push_back(c.elec ? s.charge[t] : 0.0);
+                sbond.push_back(t + 1 < s.N ? s.bcls[t] : 0);
+            }
+        }
+        Buf<int> d_type, d_bond, d_off, d_N;
+        Buf<double> d_chg, d_nv, d_blen;
+        d_type.alloc(stype.size()); upload(d_type, stype);
+        d_bond.alloc(sbond.size()); upload(d_bond, sbond);
+        d_off.alloc(soff.size()); upload(d_off, soff);
+        d_N.alloc(sN.size()); upload(d_N, sN);
+        d_chg.alloc(schg.size()); upload(d_chg, schg);
+        d_nv.alloc(snv.size()); upload(d_nv, snv);
+        std::vector<double> blen = c.bond_lengths;
+        if (blen.empty()) blen.push_back(1.0);
+        d_blen.alloc(blen.size()); upload(d_blen, blen);
+        ModeTab co{};
+        for (int a = 0; a < nm; ++a) {
+            co.c[a] = c.coeff[a];
+            co.s[a] = c.dt * c.lambda[a];
+            co.g[a] = make_double2(c.gamma[a].x * c.gamma[a].x - c.gamma[a].y * c.gamma[a].y, 0.0);   // Re(gamma^2)
+        }
+        SiOTab so{};
+        if (c.bond_lengths.size() > 8) throw std::runtime_error("semi-implicit scheme: at most 8 distinct bond lengths");
+        for (int a = 0; a < nm; ++a)
+            for (int al = 0; al < c.M; ++al) so.O[a * c.M + al] = c.O[a * c.M + al];
+        IonTab it{};
+        const int J = (int)c.ions.size();
+        for (int j = 0; j < J; ++j) {
+            it.z[j] = c.ions[j].z;
+            it.nd[j] = c.ions[j].count / c.volume;
+            it.a2[j] = c.ions[j].smear * c.ions[j].smear;
+        }
+        const int M = c.M, nsp = (int)c.sp.size(), nbc = (int)blen.size();
+        const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
+        const double a2 = c.a * c.a, lB = c.lB, dtpsi = c.dt * c.lpsi;
+        const bool elec = c.elec;
+        const double* kxp = kx.p;
+        const double* kyp = ky.p;
+        const double* kzp = kz.p;
+        const int* ty = d_type.p;
+        const int* bo = d_bond.p;
+        const int* of = d_off.p;
+        const int* Ns = d_N.p;
+        const double* ch = d_chg.p;
+        const double* nvp = d_nv.p;
+        const double* bl = d_blen.p;
+        T* P = si_P.p;
+        foreach(Vn, [=] __device__(size_t i) {
+            const int x = (int)(i / ((size_t)m2 * m3));
+            const int r = (int)(i - (size_t)x * m2 * m3);
+            const int y = r / m3, z = r - y * m3;
+            const double k2 = kxp[x] * kxp[x] + kyp[y] * kyp[y] + kzp[z] * kzp[z];
+            const double G2 = exp(-a2 * k2);   // Gamma^2
+            double phc[8];
+            for (int q = 0; q < nbc && q < 8; ++q) phc[q] = exp(-bl[q] * bl[q] * k2 / 6.0);
+            double Soo[MAXMODE], Szz = 0.0;
+            for (int a = 0; a < nm; ++a) Soo[a] = 0.0;
+            for (int sp = 0; sp < nsp; ++sp) {
+                const double w = nvp[sp];
+                double Fo[MAXMODE], Fz = 0.0;
+                for (int a = 0; a < nm; ++a) Fo[a] = 0.0;
+                const int o0 = of[sp];
+                for (int t = 0; t < Ns[sp]; ++t) {
+                    const double ph = t > 0 ? phc[bo[o0 + t - 1]] : 0.0;
+                    const int tp = ty[o0 + t];
+                    for (int a = 0; a < nm; ++a) {
+                        const double o = so.O[a * M + tp];
+                        Fo[a] *= ph;
+                        Soo[a] += w * o * (o + 2.0 * Fo[a]);
+                        Fo[a] += o;
+                    }
+                    const double zt = ch[o0 + t];
+                    Fz *= ph;
+                    Szz += w * zt * (zt + 2.0 * Fz);
+                    Fz += zt;
+                }
+            }
+            const bool k0 = k2 == 0.0;
+            for (int a = 0; a < nm; ++a) {
+                double G = co.c[a] - (k0 ? 0.0 : co.g[a].x * G2 * Soo[a]);
+                if (G < 0.0) G = 0.0;
+                P[(size_t)a * Vn + i] = (T)(1.0 / (1.0 + co.s[a] * G));
+            }
+            double Gp = 0.0;
+            if (elec && !k0) {
+                Gp = k2 / (4.0 * PI * lB) + G2 * Szz;
+                for (int j = 0; j < J; ++j) Gp += it.nd[j] * it.z[j] * it.z[j] * exp(-it.a2[j] * k2);
+            }
+            P[(size_t)nm * Vn + i] = (T)(1.0 / (1.0 + dtpsi * Gp));
+        });
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        d_type.release(); d_bond.release(); d_off.release(); d_N.release(); d_chg.release(); d_nv.release(); d_blen.release();
+    }
+
+    // increments (nm + 1 fields of si_inc) -> P * increments, in place
+    void si_precondition()
+    {
+        const size_t Vn = V_;
+        const int nf = c.nm + 1;
+        fft3<-1>(si_inc.p, nf);
+        V* inc = si_inc.p;
+        const T* P = si_P.p;
+        const T invV = (T)(1.0 / (double)Vn);
+        foreach(Vn * nf, [=] __device__(size_t i) { inc[i] = cscale(inc[i], P[i] * invV); });
+        fft3<+1>(si_inc.p, nf);
     }
 
     // ---- launch helpers ----
@@ -862,14 +1011,29 @@ struct Engine : EngineBase {
         auto qf = [&](int seg) { return qF.p + (size_t)seg * Vn; };
         double2* factor = &ds->factor[isp];
         double* qpart = part.p;
+        // renormalisation bookkeeping (see Renorm in passes.cuh)
+        const int nparts = seg_pass_ctas();
+        const size_t pslot = (size_t)std::max(c.m1, c.m1 * c.m2);
+        auto pm = [&](int s) { return pmax.p + (size_t)(s & 1) * pslot; };
+        auto rn = [&](int s) {
+            Renorm r{};
+            r.eF = expo.p;
+            r.eB = expo.p + Nmax;
+            r.nparts = nparts;
+            r.s = s;
+            r.N = N;
+            r.pmax_cur = pm(s);
+            r.pmax_prev = pm(s + 1);   // the pass before: segment s-1 (forward) or s+1 (backward), other parity
+            return r;
+        };
         // ---- forward sweep ----
         if (N == 1) {
             OpProp<T, FWD_SINGLE> op{};
-            op.E = Ec(0); op.qstore = qf(0); op.partial = reinterpret_cast<double2*>(qpart);
+            op.E = Ec(0); op.qstore = qf(0); op.partial = reinterpret_cast<double2*>(qpart); op.rn = rn(0);
             seg_pass<0, 0, FWD_SINGLE>(nullptr, nullptr, op);
         } else {
             OpProp<T, FWD_START> op0{};
-            op0.E = Ec(0); op0.qstore = qf(0);
+            op0.E = Ec(0); op0.qstore = qf(0); op0.rn = rn(0);
             seg_pass<0, -1, FWD_START>(nullptr, G.p, op0);
             for (int b = 0; b < N - 1; ++b) {
                 OpBond<T, true, false> ob{};
@@ -878,26 +1042,29 @@ struct Engine : EngineBase {
                 bond_pass<-1, +1, true, false>(G.p, H.p, ob);
                 if (b + 1 < N - 1) {
                     OpProp<T, FWD_MID> op{};
-                    op.E = Ec(b + 1); op.qstore = qf(b + 1);
+                    op.E = Ec(b + 1); op.qstore = qf(b + 1); op.rn = rn(b + 1);
                     seg_pass<+1, -1, FWD_MID>(H.p, G.p, op);
                 } else {
                     OpProp<T, FWD_LAST> op{};
                     op.E = Ec(b + 1); op.qstore = qf(b + 1); op.partial = reinterpret_cast<double2*>(qpart);
+                    op.rn = rn(b + 1);
                     seg_pass<+1, 0, FWD_LAST>(H.p, nullptr, op);
                 }
             }
         }
-        // ---- Q and the species factor (n/V)/Q ----
+        // ---- Q (of the stored, scaled qF[N-1]) and the species factor (n/V)/Q ----
         {
             const int cnt = seg_pass_ctas();
             const double nv = s.nc / c.volume;
             const double invV = 1.0 / (double)Vn;
             DevScal* d = ds;
+            const int* eF = expo.p;
+            const int last = N - 1;
             k_combine<false><<<2, 32, 0, stream>>>(qpart, cnt, 2, reinterpret_cast<double*>(&d->Q[isp]));
             k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
-                const double2 Q = dscale(d->Q[isp], invV);
-                d->Q[isp] = Q;
-                d->factor[isp] = dscale(dinv(Q), nv);
+                const double2 Qs = dscale(d->Q[isp], invV);
+                d->factor[isp] = dscale(dinv(Qs), nv);
+                d->Q[isp] = make_double2(ldexp(Qs.x, eF[last]), ldexp(Qs.y, eF[last]));   // true Q
             });
             launches += 2;
         }
@@ -907,13 +1074,14 @@ struct Engine : EngineBase {
         if (N == 1) {
             OpProp<T, BWD_SINGLE> op{};
             op.qread = qf(0); op.rho_type = rho_of(0); op.rho_charge = rchg(0); op.z = (T)s.charge[0]; op.factor = factor;
+            op.rn = rn(0);
             seg_pass<0, 0, BWD_SINGLE>(nullptr, nullptr, op);
             return;
         }
         {
             OpProp<T, BWD_START> op{};
             op.E = Ec(N - 1); op.qread = qf(N - 1); op.rho_type = rho_of(N - 1); op.rho_charge = rchg(N - 1);
-            op.z = (T)s.charge[N - 1]; op.factor = factor;
+            op.z = (T)s.charge[N - 1]; op.factor = factor; op.rn = rn(N - 1);
             seg_pass<0, +1, BWD_START>(nullptr, G.p, op);
         }
         for (int b = N - 2; b >= 0; --b) {
@@ -923,6 +1091,10 @@ struct Engine : EngineBase {
                 ob.factor = factor;
                 ob.partial = reinterpret_cast<double2*>(spart.p);
                 ob.b2 = s.bond[b] * s.bond[b];
+                ob.eF = expo.p;
+                ob.eB = expo.p + Nmax;
+                ob.s = b;
+                ob.N = N;
                 set_bond(ob, s.bcls[b]);
                 bond_pass<+1, -1, false, true>(G.p, H.p, ob);
             } else {
@@ -933,12 +1105,12 @@ struct Engine : EngineBase {
             if (b > 0) {
                 OpProp<T, BWD_MID> op{};
                 op.E = Ec(b); op.qread = qf(b); op.rho_type = rho_of(b); op.rho_charge = rchg(b);
-                op.z = (T)s.charge[b]; op.factor = factor;
+                op.z = (T)s.charge[b]; op.factor = factor; op.rn = rn(b);
                 seg_pass<-1, +1, BWD_MID>(H.p, G.p, op);
             } else {
                 OpProp<T, BWD_LAST> op{};
                 op.qread = qf(0); op.rho_type = rho_of(0); op.rho_charge = rchg(0);
-                op.z = (T)s.charge[0]; op.factor = factor;
+                op.z = (T)s.charge[0]; op.factor = factor; op.rn = rn(0);
                 seg_pass<-1, 0, BWD_LAST>(H.p, nullptr, op);
             }
         }
@@ -1211,6 +1383,39 @@ struct Engine : EngineBase {
         T* e = eta.p;
         DevScal* d = ds;
         const double invV = 1.0 / (double)Vn;
+        if (c.scheme == FTSP_SCHEME_SI) {
+            V* inc = si_inc.p;
+            foreach(Vn, [=] __device__(size_t i) {
+                T ep = e[(size_t)nm * Vn + i];
+                if (elec) {
+                    ep = (T)((double)ep + (-(d->mean_eta * invV)));
+                    e[(size_t)nm * Vn + i] = ep;
+                }
+                for (int a = 0; a < nm; ++a) {
+                    V v = cscale(u[(size_t)a * Vn + i], (T)co.s[a]);
+                    v.x += e[(size_t)a * Vn + i];
+                    inc[(size_t)a * Vn + i] = v;
+                }
+                V pv = mkc<V>(T(0), T(0));
+                if (elec) {
+                    V dv = cadd(dp[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+                    dp[i] = dv;
+                    pv = cscale(dv, (T)sp);
+                    pv.x += ep;
+                }
+                inc[(size_t)nm * Vn + i] = pv;
+            });
+            si_precondition();
+            reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
+                for (int a = 0; a < nm; ++a) ob[(size_t)a * Vn + i] = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
+                const V pv = elec ? cadd(ps[i], inc[(size_t)nm * Vn + i]) : mkc<V>(T(0), T(0));
+                pb[i] = pv;
+                acc[0] += (double)pv.x;
+                acc[1] += (double)pv.y;
+            }, reinterpret_cast<double*>(&ds->mean_psi));
+            remove_mean(psi_bar.p, &ds->mean_psi);
+            return;
+        }
         reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
             const double me = elec ? d->mean_eta * invV : 0.0;
             T ep = e[(size_t)nm * Vn + i];
@@ -1284,6 +1489,40 @@ struct Engine : EngineBase {
             if (!isfinite(v)) v = INFINITY;
             acc[nm] = fmax(acc[nm], v);
         }, ds->dmax);
+        if (c.scheme == FTSP_SCHEME_SI) {
+            V* inc = si_inc.p;
+            foreach(Vn, [=] __device__(size_t i) {
+                for (int a = 0; a < nm; ++a) {
+                    V v = cscale(cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]), (T)co.s[a]);
+                    v.x += e[(size_t)a * Vn + i];
+                    inc[(size_t)a * Vn + i] = v;
+                }
+                V pv = mkc<V>(T(0), T(0));
+                if (elec) {
+                    const V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+                    db[i] = dbv;
+                    pv = cscale(cadd(dp[i], dbv), (T)sp);
+                    pv.x += e[(size_t)nm * Vn + i];
+                }
+                inc[(size_t)nm * Vn + i] = pv;
+            });
+            si_precondition();
+            reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
+                bool bad = false;
+                for (int a = 0; a < nm; ++a) {
+                    const V w = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
+                    om[(size_t)a * Vn + i] = w;
+                    bad |= !(isfinite((double)w.x) && isfinite((double)w.y));
+                }
+                const V pv = elec ? cadd(ps[i], inc[(size_t)nm * Vn + i]) : mkc<V>(T(0), T(0));
+                ps[i] = pv;
+                acc[0] += (double)pv.x;
+                acc[1] += (double)pv.y;
+                if (bad || !(isfinite((double)pv.x) && isfinite((double)pv.y))) acc[2] += 1.0;
+            }, ds->corr);
+            remove_mean(psi.p, reinterpret_cast<const double2*>(ds->corr));
+            return;
+        }
         reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
             bool bad = false;
             for (int a = 0; a < nm; ++a) {
@@ -1522,6 +1761,11 @@ struct Engine : EngineBase {
         } else {
             FTSP_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(V) * Vn, stream));
         }
+        FTSP_CUDA(cudaMemsetAsync(&ds->bad_last, 0, sizeof(int), stream));
+        if (c.restart_interval > 0) {
+            if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(ck.p, omega.p, sizeof(V) * nm * Vn, cudaMemcpyDeviceToDevice, stream));
+            FTSP_CUDA(cudaMemcpyAsync(ck.p + (size_t)nm * Vn, psi.p, sizeof(V) * Vn, cudaMemcpyDeviceToDevice, stream));
+        }
         FTSP_CUDA(cudaStreamSynchronize(stream));
     }
 
@@ -1548,14 +1792,31 @@ struct Engine : EngineBase {
         else if (name == "W_type_s") { p = kB.p; n = (size_t)M * Vn; }
         else if (name == "psi_s") { p = kB.p + (size_t)M * Vn; n = Vn; }
         else if (name == "qF") { p = qF.p; n = (size_t)Nmax * Vn; }
+        else if (name == "si_precond" && si_P.p) {
+            const size_t nr = (size_t)(nm + 1) * Vn;
+            if (out) {
+                std::vector<T> tmp(nr);
+                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), si_P.p, sizeof(T) * nr, cudaMemcpyDeviceToHost, stream));
+                FTSP_CUDA(cudaStreamSynchronize(stream));
+                for (size_t i = 0; i < nr; ++i) {
+                    out[2 * i] = (double)tmp[i];
+                    out[2 * i + 1] = 0.0;
+                }
+            }
+            return (long long)(2 * nr);
+        }
         else return -1;
         if (out && n) {
             std::vector<V> tmp(n);
             FTSP_CUDA(cudaMemcpyAsync(tmp.data(), p, sizeof(V) * n, cudaMemcpyDeviceToHost, stream));
+            std::vector<int> ex((size_t)Nmax, 0);
+            if (name == "qF") FTSP_CUDA(cudaMemcpyAsync(ex.data(), expo.p, sizeof(int) * Nmax, cudaMemcpyDeviceToHost, stream));
             FTSP_CUDA(cudaStreamSynchronize(stream));
             for (size_t i = 0; i < n; ++i) {
-                out[2 * i] = (double)tmp[i].x;
-                out[2 * i + 1] = (double)tmp[i].y;
+                // qF is stored renormalised by 2^-aF[s]; return the true propagator
+                const int e2 = name == "qF" ? ex[i / Vn] : 0;
+                out[2 * i] = std::ldexp((double)tmp[i].x, e2);
+                out[2 * i + 1] = std::ldexp((double)tmp[i].y, e2);
             }
         }
         return (long long)(2 * n);
@@ -1613,8 +1874,64 @@ struct Engine : EngineBase {
         noise_injected = true;
     }
 
+    // ---- device-side checkpoint and rollback (complexLangevin.cu:583-636 semantics) ----
+    // A step that ends with a non-finite field, Q or observable sets bad_last;
+    // the next step first restores (omega, psi) from the last checkpoint and
+    // counts a restart.  Checkpoints are taken every restart_interval steps
+    // from a finite state.  Everything stays on the device.
+    void restore_if_bad()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        V* om = omega.p;
+        V* ps = psi.p;
+        const V* ckp = ck.p;
+        DevScal* d = ds;
+        foreach(Vn, [=] __device__(size_t i) {
+            if (!d->bad_last) return;
+            for (int a = 0; a < nm; ++a) om[(size_t)a * Vn + i] = ckp[(size_t)a * Vn + i];
+            ps[i] = ckp[(size_t)nm * Vn + i];
+        });
+        k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+            if (d->bad_last) {
+                d->restarts += 1;
+                d->bad_last = 0;
+            }
+        });
+        ++launches;
+    }
+
+    void mark_step_status()
+    {
+        DevScal* d = ds;
+        const int S = (int)c.sp.size(), R = c.record_len();
+        k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+            bool bad = d->nonfinite != 0 || d->corr[2] != 0.0;
+            for (int s = 0; s < S; ++s) bad |= !(isfinite(d->Q[s].x) && isfinite(d->Q[s].y));
+            for (int i = 0; i < 2 * R; ++i) bad |= !isfinite(d->rec[i]);
+            d->bad_last = bad ? 1 : 0;
+        });
+        ++launches;
+    }
+
+    void checkpoint_if_good()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        const V* om = omega.p;
+        const V* ps = psi.p;
+        V* ckp = ck.p;
+        const DevScal* d = ds;
+        foreach(Vn, [=] __device__(size_t i) {
+            if (d->bad_last) return;
+            for (int a = 0; a < nm; ++a) ckp[(size_t)a * Vn + i] = om[(size_t)a * Vn + i];
+            ckp[(size_t)nm * Vn + i] = ps[i];
+        });
+    }
+
     void step_device()
     {
+        if (c.restart_interval > 0) restore_if_bad();
         const bool st = c.stress_on();
         eval(0, false);
         // save Q of the first evaluation for the finite check
@@ -1637,6 +1954,8 @@ struct Engine : EngineBase {
         finalize_record(st);
         corrector();
         ++step_counter;
+        mark_step_status();
+        if (c.restart_interval > 0 && step_counter % (uint64_t)c.restart_interval == 0) checkpoint_if_good();
     }
 
     int status_from_host()
@@ -1750,6 +2069,12 @@ struct Engine : EngineBase {
             Qh[0] = q[0] / (double)Vn;
             Qh[1] = q[1] / (double)Vn;
         }
+    }
+
+    long long restarts() override
+    {
+        pull_scalars();
+        return hs.restarts;
     }
 
     void views(ftsp_views* v) override

@@ -302,6 +302,46 @@ struct OpIdentity {
     __device__ __forceinline__ void end(double*, size_t) {}
 };
 
+// Power-of-two renormalisation of the propagators (all optional: a null eF
+// turns it off).  Each real-space segment pass records, per CTA, the largest
+// component magnitude of the propagator it wrote (pmax_cur); the next pass of
+// the same sweep reduces those maxima, scales its output by 2^-d with
+// d = floor(log2 max), and accumulates d into a per-segment exponent:
+//   qF[s] is stored as qF_true[s] 2^-aF[s],  qB[s] as qB_true[s] 2^-aB[s].
+// Scaling by powers of two is exact in binary floating point, so complex128
+// results are unchanged while complex64 propagators stay in range.  A density
+// or stress contribution of segment s then carries 2^(aF[s] + aB[s+1] - aF[N-1])
+// (the partition function is Q_true = mean(qF[N-1]) 2^aF[N-1]).
+struct Renorm {
+    int* eF;                 // forward exponents aF[0..N) (null: no renormalisation)
+    int* eB;                 // backward exponents aB[0..N)
+    const float* pmax_prev;  // per-CTA maxima written by the previous pass of this sweep
+    float* pmax_cur;         // per-CTA maxima of this pass
+    int nparts;              // number of entries of pmax_prev
+    int s;                   // segment index of this pass
+    int N;                   // segments of the species
+};
+
+__device__ __forceinline__ int reduce_exponent(const float* pm, int n)
+{
+    __shared__ float s_red[32];
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, pm[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = 0.0f;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) r = fmaxf(r, s_red[w]);
+        s_red[0] = r;
+    }
+    __syncthreads();
+    const float M = s_red[0];
+    __syncthreads();
+    return (M > 0.0f && isfinite(M)) ? ilogbf(M) : 0;
+}
+
 // Chain-propagator pointwise work in the real-space pass of one segment.
 // KIND selects the sweep position:
 //   forward : q = u * E (u = IFFT of the previous bond, or 1 at s = 0);
@@ -321,14 +361,18 @@ struct OpProp {
     V* rho_type;             // backward: density accumulator of the segment's type
     V* rho_charge;           // backward: charge accumulator (null when z == 0)
     T z;                     // segment valence
-    const double2* factor;   // backward: species factor (n/V)/Q
+    const double2* factor;   // backward: species factor (n/V)/Q (Q of the stored, scaled qF)
     double2* partial;        // forward last: per-CTA sums of q
+    Renorm rn;               // renormalisation (rn.eF null: off)
     double acc[2];
-    T fr, fi;
+    float amax;
+    T fr, fi;                // density factor (with the segment's exponent folded in)
+    T oscale;                // output scale 2^-d
 
     static constexpr bool FWD = KIND <= FWD_SINGLE;
     static constexpr bool NEED_E = KIND == FWD_START || KIND == FWD_MID || KIND == FWD_LAST || KIND == FWD_SINGLE ||
                                    KIND == BWD_START || KIND == BWD_MID;
+    static constexpr bool MAX_OUT = KIND == FWD_START || KIND == FWD_MID || KIND == BWD_START || KIND == BWD_MID;
     struct Pre {
         V e, q, r, c;
     };
@@ -336,10 +380,32 @@ struct OpProp {
     __device__ __forceinline__ void begin()
     {
         acc[0] = acc[1] = 0.0;
+        amax = 0.0f;
+        oscale = T(1);
+        int dens_exp = 0;
+        if (rn.eF) {
+            const bool first = blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0;
+            if (KIND == FWD_START || KIND == FWD_SINGLE) {
+                if (first) rn.eF[0] = 0;
+            } else if (KIND == FWD_MID || KIND == FWD_LAST) {
+                const int d = reduce_exponent(rn.pmax_prev, rn.nparts);
+                oscale = (T)ldexp(1.0, -d);
+                if (first) rn.eF[rn.s] = rn.eF[rn.s - 1] + d;
+            } else if (KIND == BWD_START || KIND == BWD_SINGLE) {
+                if (first) rn.eB[rn.s] = 0;
+            } else if (KIND == BWD_MID) {
+                const int d = reduce_exponent(rn.pmax_prev, rn.nparts);
+                oscale = (T)ldexp(1.0, -d);
+                if (first) rn.eB[rn.s] = rn.eB[rn.s + 1] + d;
+                dens_exp = rn.eF[rn.s] + rn.eB[rn.s + 1] - rn.eF[rn.N - 1];
+            } else {   // BWD_LAST (s = 0)
+                dens_exp = rn.eF[0] + rn.eB[1] - rn.eF[rn.N - 1];
+            }
+        }
         if (!FWD) {
             const double2 fc = *factor;
-            fr = T(fc.x);
-            fi = T(fc.y);
+            fr = T(ldexp(fc.x, dens_exp));
+            fi = T(ldexp(fc.y, dens_exp));
         }
     }
     __device__ __forceinline__ Pre load(int, size_t g) const
@@ -353,11 +419,17 @@ struct OpProp {
         }
         return p;
     }
+    __device__ __forceinline__ void track(V q)
+    {
+        if (MAX_OUT) amax = fmaxf(amax, fmaxf(fabsf((float)q.x), fabsf((float)q.y)));
+    }
     __device__ __forceinline__ V apply(int, int, int, int, size_t g, V u, const Pre& p)
     {
         if (FWD) {
-            const V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? p.e : cmul(u, p.e);
+            V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? p.e : cmul(u, p.e);
+            if (KIND == FWD_MID || KIND == FWD_LAST) q = cscale(q, oscale);
             qstore[g] = q;
+            track(q);
             if (KIND == FWD_LAST || KIND == FWD_SINGLE) {
                 acc[0] += (double)q.x;
                 acc[1] += (double)q.y;
@@ -368,8 +440,15 @@ struct OpProp {
             const V w = cmul(phi, mkc<V>(fr, fi));
             rho_type[g] = cadd(p.r, w);
             if (rho_charge) rho_charge[g] = cadd(p.c, cscale(w, z));
-            if (KIND == BWD_START) return p.e;
-            if (KIND == BWD_MID) return cmul(u, p.e);
+            if (KIND == BWD_START) {
+                track(p.e);
+                return p.e;
+            }
+            if (KIND == BWD_MID) {
+                const V q = cscale(cmul(u, p.e), oscale);
+                track(q);
+                return q;
+            }
             return u;
         }
     }
@@ -379,6 +458,20 @@ struct OpProp {
             __syncthreads();
             block_sum<2>(acc, scratch);
             if (threadIdx.x == 0) partial[cta] = make_double2(acc[0], acc[1]);
+        }
+        if (MAX_OUT && rn.eF) {
+            __syncthreads();
+            float* sm = reinterpret_cast<float*>(scratch);
+            float m = amax;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float r = 0.0f;
+                for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) r = fmaxf(r, sm[w]);
+                rn.pmax_cur[cta] = r;
+            }
         }
     }
 };
@@ -406,6 +499,9 @@ struct OpBond {
     double b2;
     const double2* factor;
     double2* partial;        // [cta][6] accumulated across bonds
+    const int* eF;           // renormalisation exponents (null: off)
+    const int* eB;
+    int s, N;                // bond s -> s+1 of a species with N segments
     double acc[12];
     struct Pre {
         V F;
@@ -450,9 +546,10 @@ struct OpBond {
             block_sum<12>(acc, scratch);
             if (threadIdx.x == 0) {
                 const double2 fc = *factor;
+                const double w = eF ? ldexp(b2, eF[s] + eB[s + 1] - eF[N - 1]) : b2;
 #pragma unroll
                 for (int c = 0; c < 6; ++c) {
-                    const double sr = b2 * acc[2 * c], si = b2 * acc[2 * c + 1];
+                    const double sr = w * acc[2 * c], si = w * acc[2 * c + 1];
                     double2 o = partial[cta * 6 + c];
                     o.x += sr * fc.x - si * fc.y;
                     o.y += sr * fc.y + si * fc.x;

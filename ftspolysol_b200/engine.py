@@ -47,7 +47,7 @@ class ftsp_config(C.Structure):
         ("ion_smear", C.POINTER(C.c_double)),
         ("self_pressure", C.c_double), ("stress_mask", C.c_int), ("isotropic_pressure", C.c_int),
         ("noise", C.c_int), ("seed", C.c_ulonglong), ("precision", C.c_int), ("scheme", C.c_int),
-        ("device", C.c_int),
+        ("device", C.c_int), ("restart_interval", C.c_int),
     ]
 
 
@@ -97,6 +97,8 @@ def lib():
         L.ftsp_last_launch_count.restype = C.c_longlong
         L.ftsp_last_launch_count.argtypes = [vp]
         L.ftsp_propagate_chain.argtypes = [vp, vp, C.c_int, C.c_double, vp, vp]
+        L.ftsp_restart_count.restype = C.c_longlong
+        L.ftsp_restart_count.argtypes = [vp]
         L.ftsp_propagate_chain_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                                    vp, C.c_int, C.c_double, vp, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
@@ -110,7 +112,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
-               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc")
+               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count")
 
 
 def _dp(a):
@@ -154,7 +156,7 @@ class Engine:
     """
 
     def __init__(self, derived: dict, precision: int = FP64, scheme: int = SCHEME_PC, noise: bool = False,
-                 seed: int = 0, device: int = 0):
+                 seed: int = 0, device: int = 0, restart_interval: int = 0):
         L = lib()
         self._keep = []
 
@@ -213,6 +215,7 @@ class Engine:
         cfg.precision = int(precision)
         cfg.scheme = int(scheme)
         cfg.device = int(device)
+        cfg.restart_interval = int(restart_interval)
         self.precision = precision
         self._cfg = cfg
         h = C.c_void_p()
@@ -321,6 +324,9 @@ class Engine:
 
     def set_stream(self, stream_handle: int):
         self._check(lib().ftsp_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def restarts(self) -> int:
+        return int(lib().ftsp_restart_count(self.h))
 
     def launches(self) -> int:
         return int(lib().ftsp_last_launch_count(self.h))

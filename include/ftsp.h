@@ -77,6 +77,10 @@ typedef struct ftsp_config {
     int precision;               /* FTSP_FP64 or FTSP_FP32                            */
     int scheme;                  /* FTSP_SCHEME_PC or FTSP_SCHEME_SI                  */
     int device;                  /* CUDA device ordinal                               */
+    int restart_interval;        /* >0: device checkpoint every so many steps and
+                                    rollback after a non-finite step (the
+                                    reference's Ntmp / max_nan_restarts recovery,
+                                    complexLangevin.cu:583-636); 0: off          */
 } ftsp_config;
 
 typedef struct ftsp_handle ftsp_handle;
@@ -163,6 +167,10 @@ int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_len
  * finished the call's work. */
 int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, double L3, const double* w, int N,
                                  double bond_length, double* q_end, double* Q, void* cuda_stream);
+
+/* Number of checkpoint rollbacks taken so far (restart_interval > 0);
+ * -1 on error.  Synchronises the handle's stream. */
+long long ftsp_restart_count(ftsp_handle* h);
 
 /* Device pointers of the resident state (FP64 handles only), in the layout of
  * deviceState (deviceState.h:6-48). */

@@ -343,12 +343,22 @@ int timing(int argc, char** argv)
     complexLangevin cl(s.p, s.poly, s.ions);
     if (!cl.initialize(s.omega, s.psi, s.Gamma, s.PHI, s.k2, s.ion_kernels)) return 1;
     const auto t1 = std::chrono::steady_clock::now();
+    // A step that ends non-finite is followed by a restore of the input
+    // fields (the reference's checkpoint restart, complexLangevin.cu:626-636,
+    // taken from memory instead of the checkpoint files) so that the timed
+    // sample keeps running; restarts are counted and reported.
     int step = 0;
+    int restarts = 0;
+    auto restore = [&]() {
+        copy_to_device(cl.d.omega, s.omega);
+        copy_to_device(cl.d.psi, s.psi);
+        cl.remove_psi_zero_mode(cl.d.psi);
+        ++restarts;
+    };
     for (int i = 0; i < warmup; ++i) {
-        if (cl.run_step(false, ++step) != complexLangevin::StepStatus::ok) {
-            std::fprintf(stderr, "harness: warm-up step %d did not finish ok\n", step);
-            return 1;
-        }
+        const auto st = cl.run_step(false, ++step);
+        if (st == complexLangevin::StepStatus::failed) return 1;
+        if (st == complexLangevin::StepStatus::nonfinite) restore();
     }
     CUDA_CHECK(cudaDeviceSynchronize());
     cudaEvent_t e0, e1;
@@ -357,10 +367,9 @@ int timing(int argc, char** argv)
     const auto w0 = std::chrono::steady_clock::now();
     CUDA_CHECK(cudaEventRecord(e0));
     for (int i = 0; i < steps; ++i) {
-        if (cl.run_step(false, ++step) != complexLangevin::StepStatus::ok) {
-            std::fprintf(stderr, "harness: timed step %d did not finish ok\n", step);
-            return 1;
-        }
+        const auto st = cl.run_step(false, ++step);
+        if (st == complexLangevin::StepStatus::failed) return 1;
+        if (st == complexLangevin::StepStatus::nonfinite) restore();
     }
     CUDA_CHECK(cudaEventRecord(e1));
     CUDA_CHECK(cudaEventSynchronize(e1));
@@ -370,9 +379,10 @@ int timing(int argc, char** argv)
     const double wall = std::chrono::duration<double>(w1 - w0).count();
     const double setup_s = std::chrono::duration<double>(t1 - t0).count();
     std::printf("{\"impl\": \"reference-cuda\", \"grid\": [%d, %d, %d], \"N\": %d, \"steps\": %d, \"warmup\": %d, "
-                "\"event_ms_per_step\": %.6f, \"wall_ms_per_step\": %.6f, \"steps_per_s\": %.6f, \"setup_s\": %.3f}\n",
+                "\"event_ms_per_step\": %.6f, \"wall_ms_per_step\": %.6f, \"steps_per_s\": %.6f, \"setup_s\": %.3f, "
+                "\"restarts\": %d}\n",
                 s.p.m1, s.p.m2, s.p.m3, s.p.Nmax, steps, warmup, ms / steps, 1e3 * wall / steps,
-                steps / (ms * 1e-3), setup_s);
+                steps / (ms * 1e-3), setup_s, restarts);
     return 0;
 }
 
