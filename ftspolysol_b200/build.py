@@ -20,7 +20,10 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libftsp.so")
 
 SOURCES = ["engine_f32.cu", "engine_f64.cu", "abi.cu"]
-HEADERS = ["fft_core.cuh", "passes.cuh", "engine.cuh"]
+HOST_SOURCES = ["host_model.cpp", "host_io.cpp", "host_run.cpp"]
+HEADERS = ["fft_core.cuh", "passes.cuh", "engine.cuh", "host_model.h", "host_io.h"]
+MAIN = os.path.join(HERE, "ftsp_main")
+HOST_FLAGS = ["-O2", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-Wall"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-O2",
          "-Xptxas", "-warn-spills"]
@@ -35,7 +38,10 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "ftsp.h")]
+    if not os.path.exists(MAIN) or os.path.getmtime(MAIN) < t:
+        return True
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HOST_SOURCES + HEADERS + ["main.cpp"]]
+    deps += [os.path.join(INCLUDE, h) for h in ("ftsp.h", "ftsp_host.h")]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
@@ -47,10 +53,11 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     os.makedirs(objdir, exist_ok=True)
     procs = []
     objs = []
-    for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+    for src in SOURCES + HOST_SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
-        cmd = [nvcc()] + ARCH + FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        flags = ARCH + FLAGS if src.endswith(".cu") else HOST_FLAGS
+        cmd = [nvcc()] + flags + ["-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
         if extra:
             cmd += list(extra)
         if verbose:
@@ -72,6 +79,14 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("linking libftsp.so failed")
     os.replace(LIB + ".tmp", LIB)
+    # the reference-style executable: a thin main() over ftsp_main()
+    exe = [nvcc(), "-O2", "-std=c++17", "-I", INCLUDE, os.path.join(CSRC, "main.cpp"), "-o", MAIN + ".tmp",
+           "-L", HERE, "-lftsp", "-Xlinker", "-rpath,$ORIGIN"]
+    res = subprocess.run(exe, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("linking ftsp_main failed")
+    os.replace(MAIN + ".tmp", MAIN)
     return LIB
 
 
