@@ -385,7 +385,7 @@ extern "C" int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, d
         const int ms[3] = {m1, m2, m3};
         const double Ls[3] = {L1, L2, L3};
         for (int d = 0; d < 3; ++d) {
-            ht.plans[d] = make_plan(ms[d]);
+            ht.plans[d] = make_plan(ms[d], 3);   // complex128: radix <= 8
             for (int j = 0; j < ms[d]; ++j) {
                 const long double ang = -2.0L * 3.141592653589793238462643383279502884L * j / ms[d];
                 ht.tw[d][j] = make_double2((double)cosl(ang), (double)sinl(ang));

@@ -117,7 +117,10 @@ struct HostCfg {
 // Radix plan: the power-of-two part in as few stages of radix <= 16 as
 // possible, spread evenly (128 = 16 x 8, 64 = 8 x 8, 32 = 8 x 4), then the
 // factors 3 and 5.
-static FftPlan1 make_plan(int n)
+// max_bits: largest power-of-two radix as a bit count (4: radix 16 for
+// complex64, 3: radix 8 for complex128, whose line passes hold 8 values per
+// thread).
+static FftPlan1 make_plan(int n, int max_bits)
 {
     FftPlan1 p{};
     p.n = n;
@@ -127,7 +130,7 @@ static FftPlan1 make_plan(int n)
         r /= 2;
         ++p2;
     }
-    const int nst2 = (p2 + 3) / 4;
+    const int nst2 = (p2 + max_bits - 1) / max_bits;
     int left = p2;
     for (int st = 0; st < nst2; ++st) {
         const int bits = (left + (nst2 - st) - 1) / (nst2 - st);   // ceil(bits left / stages left)
@@ -556,7 +559,8 @@ struct Engine : EngineBase {
         int dev_smem = 0;
         FTSP_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
         pg.m1 = m1; pg.m2 = m2; pg.m3 = m3; pg.P = m3 + 1;
-        const FftPlan1 hp[3] = {make_plan(m1), make_plan(m2), make_plan(m3)};
+        const int max_bits = F32 ? 4 : 3;
+        const FftPlan1 hp[3] = {make_plan(m1, max_bits), make_plan(m2, max_bits), make_plan(m3, max_bits)};
         plans.alloc(3);
         FTSP_CUDA(cudaMemcpy(plans.p, hp, sizeof(hp), cudaMemcpyHostToDevice));
         pg.py = plans.p + 1;

@@ -267,7 +267,7 @@ __device__ __forceinline__ void fft_tile(V* tile, const V* __restrict__ tw, cons
         const unsigned span = p->span[st], tstep = p->tstep[st];
         const FastDiv fs = p->fspan[st];
         switch (p->rad[st]) {
-        case 16: if constexpr (E >= 16) fft_stage<V, S, 16, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
+        case 16: fft_stage<V, S, 16, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
         case 8: fft_stage<V, S, 8, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
         case 4: fft_stage<V, S, 4, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;
         case 2: fft_stage<V, S, 2, E>(tile, tw, n, B, fB, js, bs, span, fs, tstep); break;

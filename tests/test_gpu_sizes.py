@@ -33,7 +33,10 @@ def rec_err(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-3)))
 
 
-GRIDS = [((32, 32, 32), 8), ((64, 64, 64), 6), ((128, 32, 32), 6), ((32, 64, 64), 5), ((128, 128, 128), 3)]
+GRIDS = [((32, 32, 32), 8), ((64, 64, 64), 6), ((128, 32, 32), 6), ((32, 64, 64), 5), ((128, 128, 128), 3),
+         # runtime-plan passes with radix-16 lengths along x and y (16, 128, 256)
+         # and mixed 2/3/5 factors
+         ((16, 12, 8), 4), ((128, 24, 20), 3), ((48, 16, 30), 3), ((256, 10, 9), 2)]
 
 
 @pytest.mark.parametrize("m,N", GRIDS)
