@@ -224,6 +224,75 @@ int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max)
     return st;
 }
 
+int ftsp_set_dt(ftsp_handle* h, double dt)
+{
+    FTSP_GUARD(h, h->eng->set_dt(dt));
+    return FTSP_OK;
+}
+
+int ftsp_learn_configure(ftsp_handle* h, const ftsp_learn_config* cfg)
+{
+    if (!cfg) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->learn_configure(*cfg));
+    return FTSP_OK;
+}
+
+int ftsp_learn_collect(ftsp_handle* h, int on)
+{
+    FTSP_GUARD(h, h->eng->learn_collect(on != 0));
+    return FTSP_OK;
+}
+
+int ftsp_learn_reset(ftsp_handle* h)
+{
+    FTSP_GUARD(h, h->eng->learn_reset());
+    return FTSP_OK;
+}
+
+int ftsp_learn_train(ftsp_handle* h, int iterations, double* loss)
+{
+    double l = 0.0;
+    FTSP_GUARD(h, l = h->eng->learn_train(iterations));
+    if (loss) *loss = l;
+    return FTSP_OK;
+}
+
+int ftsp_learn_use(ftsp_handle* h, int on)
+{
+    FTSP_GUARD(h, h->eng->learn_use(on != 0));
+    return FTSP_OK;
+}
+
+int ftsp_learn_get_stats(ftsp_handle* h, ftsp_learn_stats* st)
+{
+    if (!st) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->learn_stats(st));
+    return FTSP_OK;
+}
+
+int ftsp_learn_get_weights(ftsp_handle* h, float* out, int* n)
+{
+    if (!n) return FTSP_ERROR;
+    FTSP_GUARD(h, *n = h->eng->learn_weights(out, out ? *n : 0, false));
+    return FTSP_OK;
+}
+
+int ftsp_learn_set_weights(ftsp_handle* h, const float* w, int n)
+{
+    if (!w) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->learn_weights(const_cast<float*>(w), n, true));
+    return FTSP_OK;
+}
+
+int ftsp_learn_grad(ftsp_handle* h, const float* x, const float* t, const float* m, int n, double* loss, float* grad)
+{
+    if (!x || !t || !m || !grad) return FTSP_ERROR;
+    double l = 0.0;
+    FTSP_GUARD(h, l = h->eng->learn_grad(x, t, m, n, grad));
+    if (loss) *loss = l;
+    return FTSP_OK;
+}
+
 int ftsp_state_views(ftsp_handle* h, ftsp_views* v)
 {
     if (!v) return FTSP_ERROR;

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "passes.cuh"
+#include "learned.cuh"
 #include "ftsp.h"
 
 namespace ftsp {
@@ -61,9 +62,14 @@ struct DevScal {
     alignas(16) double sconn[12];          // connectivity stress sums over the bond-pass CTAs
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
+    alignas(16) double lres[2];            // learned preconditioner: force residuals (learned, analytic) of the step
+    alignas(16) double lres_sum[2];        // and their sums since the last statistics reset
     alignas(16) int nonfinite;
     int bad_last;                          // the last step produced a non-finite value
     int restarts;                          // checkpoint rollbacks so far
+    int lr_use;                            // the next step preconditions with the learned G(k)
+    int lr_checks;                         // steps judged by the residual test
+    int lr_fallbacks;                      // of those, steps that fell back to the analytic G(k)
 };
 static_assert(offsetof(DevScal, rec) % 16 == 0 && offsetof(DevScal, corr) % 16 == 0, "DevScal alignment");
 
@@ -361,6 +367,34 @@ struct ProfStat {
     double bytes = 0.0;   // algorithmic bytes (minimum HBM traffic of the launch's work)
 };
 
+// Features of wave vector i for the learned preconditioner's network
+// (learned.cuh): log(1 + k^2), log(1 + P_w), log(1 + P_psi), N / 50, lB,
+// 10 c_salt.
+struct LearnFeat {
+    const double* kx;
+    const double* ky;
+    const double* kz;
+    const float* Pw;
+    const float* Pp;
+    int m2, m3;
+    float N, lB, salt;
+    __device__ __forceinline__ bool operator()(size_t i, float* x) const
+    {
+        const size_t yz = (size_t)m2 * m3;
+        const int ix = (int)(i / yz);
+        const int r = (int)(i - (size_t)ix * yz);
+        const int iy = r / m3, iz = r - iy * m3;
+        const double k2 = kx[ix] * kx[ix] + ky[iy] * ky[iy] + kz[iz] * kz[iz];
+        x[0] = (float)log1p(k2);
+        x[1] = log1pf(fmaxf(Pw[i], 0.0f));
+        x[2] = log1pf(fmaxf(Pp[i], 0.0f));
+        x[3] = N / 50.0f;
+        x[4] = lB;
+        x[5] = 10.0f * salt;
+        return true;
+    }
+};
+
 struct EngineBase {
     HostCfg c;
     std::string err;
@@ -451,6 +485,15 @@ struct EngineBase {
     virtual void views(ftsp_views* v) = 0;
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
     virtual long long restarts() = 0;
+    virtual void set_dt(double dt) = 0;
+    virtual void learn_configure(const ftsp_learn_config& cf) = 0;
+    virtual void learn_collect(bool on) = 0;
+    virtual void learn_reset() = 0;
+    virtual double learn_train(int iterations) = 0;
+    virtual void learn_use(bool on) = 0;
+    virtual void learn_stats(ftsp_learn_stats* st) = 0;
+    virtual int learn_weights(float* out, int n, bool set) = 0;
+    virtual double learn_grad(const float* x, const float* t, const float* m, int n, float* grad) = 0;
 };
 
 template <typename T>
@@ -502,7 +545,7 @@ struct Engine : EngineBase {
     Buf<V> qF, Fst, G, H;
     Buf<double> part;    // reduction partials
     Buf<int> expo;       // propagator renormalisation exponents: forward [Nmax], backward [Nmax]
-    Buf<T> si_P;         // semi-implicit preconditioner 1/(1 + lambda dt G(k)): modes, then psi
+    Buf<T> si_G;         // semi-implicit linear-response coefficients G(k) (analytic): modes, then psi
     Buf<V> si_inc;       // semi-implicit increments (nm + 1 fields)
     Buf<V> ck;           // device checkpoint of (omega, psi) for rollback
     Buf<float> pmax;     // per-CTA propagator maxima, two slots (ping-pong by segment parity)
@@ -531,7 +574,8 @@ struct Engine : EngineBase {
         plans.release();
         kx.release(); ky.release(); kz.release(); phi.release(); gam.release(); gion.release(); eta.release();
         part.release(); spart.release(); stage.release(); expo.release(); pmax.release();
-        si_P.release(); si_inc.release(); ck.release();
+        si_G.release(); si_inc.release(); ck.release();
+        learn_release();
         if (ds) cudaFree(ds);
         release_events();
     }
@@ -691,7 +735,7 @@ struct Engine : EngineBase {
     {
         const size_t Vn = V_;
         const int nm = c.nm;
-        si_P.alloc((size_t)(nm + 1) * Vn);
+        si_G.alloc((size_t)(nm + 1) * Vn);
         si_inc.alloc((size_t)(nm + 1) * Vn);
         // segment data: per segment (type, charge, bond class of the bond to the next segment)
         std::vector<int> stype, sbond, soff, sN;
@@ -736,7 +780,7 @@ struct Engine : EngineBase {
         }
         const int M = c.M, nsp = (int)c.sp.size(), nbc = (int)blen.size();
         const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
-        const double a2 = c.a * c.a, lB = c.lB, dtpsi = c.dt * c.lpsi;
+        const double a2 = c.a * c.a, lB = c.lB;
         const bool elec = c.elec;
         const double* kxp = kx.p;
         const double* kyp = ky.p;
@@ -748,7 +792,7 @@ struct Engine : EngineBase {
         const double* ch = d_chg.p;
         const double* nvp = d_nv.p;
         const double* bl = d_blen.p;
-        T* P = si_P.p;
+        T* P = si_G.p;
         foreach(Vn, [=] __device__(size_t i) {
             const int x = (int)(i / ((size_t)m2 * m3));
             const int r = (int)(i - (size_t)x * m2 * m3);
@@ -783,30 +827,421 @@ struct Engine : EngineBase {
             for (int a = 0; a < nm; ++a) {
                 double G = co.c[a] - (k0 ? 0.0 : co.g[a].x * G2 * Soo[a]);
                 if (G < 0.0) G = 0.0;
-                P[(size_t)a * Vn + i] = (T)(1.0 / (1.0 + co.s[a] * G));
+                P[(size_t)a * Vn + i] = (T)G;
             }
             double Gp = 0.0;
             if (elec && !k0) {
                 Gp = k2 / (4.0 * PI * lB) + G2 * Szz;
                 for (int j = 0; j < J; ++j) Gp += it.nd[j] * it.z[j] * it.z[j] * exp(-it.a2[j] * k2);
             }
-            P[(size_t)nm * Vn + i] = (T)(1.0 / (1.0 + dtpsi * Gp));
+            P[(size_t)nm * Vn + i] = (T)Gp;
         });
         FTSP_CUDA(cudaStreamSynchronize(stream));
         d_type.release(); d_bond.release(); d_off.release(); d_N.release(); d_chg.release(); d_nv.release(); d_blen.release();
     }
 
-    // increments (nm + 1 fields of si_inc) -> P * increments, in place
-    void si_precondition()
+    // increments (nm + 1 fields of si_inc) -> P * increments, in place, with
+    // P_f(k) = 1 / (1 + dt lambda_f G_f(k)) from the analytic table, or from
+    // the learned one while the residual test allows it (device flag lr_use).
+    // stash: keep the k-space increments FFT[omega_bar - omega] for the
+    // learned preconditioner's statistics and residual test.
+    void si_precondition(bool stash = false)
     {
         const size_t Vn = V_;
         const int nf = c.nm + 1;
         fft3<-1>(si_inc.p, nf);
         V* inc = si_inc.p;
-        const T* P = si_P.p;
+        const T* GA = si_G.p;
+        const T* GL = lr.on_use ? lr.GL.p : nullptr;
+        V* dw = stash ? lr.dw.p : nullptr;
+        SigTab st{};
+        for (int a = 0; a < c.nm; ++a) st.s[a] = c.dt * c.lambda[a];
+        st.s[c.nm] = c.dt * c.lpsi;
+        const DevScal* d = ds;
         const T invV = (T)(1.0 / (double)Vn);
-        foreach(Vn * nf, [=] __device__(size_t i) { inc[i] = cscale(inc[i], P[i] * invV); });
+        foreach(Vn * nf, [=] __device__(size_t i) {
+            const int f = (int)(i / Vn);
+            const T G = (GL && d->lr_use) ? GL[i] : GA[i];
+            const V k = cscale(inc[i], (T)(1.0 / (1.0 + st.s[f] * (double)G)));
+            if (dw) dw[i] = k;
+            inc[i] = cscale(k, invV);
+        });
         fft3<+1>(si_inc.p, nf);
+    }
+
+    // ---- learned semi-implicit preconditioner (learned.cuh) ----
+    struct Learn {
+        bool configured = false, on_collect = false, on_use = false, trained = false;
+        int nout = 0, np = 0, nb = 0;
+        float N = 50.0f, lB = 1.0f, salt = 0.0f;
+        double lr = 1e-3, fallback = 1.5;
+        int batch = 4096, refresh_every = 100;
+        uint64_t seed = 7;
+        long long collected = 0, power_updates = 0, since_refresh = 0;
+        int adam_t = 0;
+        double last_loss = 0.0;
+        Buf<float> A, B, Pw, Pp;      // statistics: <Re(du dw*)>, <|dw|^2> per field and k; spectral powers
+        Buf<T> GL;                    // learned G(k): modes, then psi
+        Buf<V> dw, du, fk;            // k-space increments, drift changes, field transforms
+        Buf<float> w, m1, m2, partial;
+        Buf<double> lpart, loss;
+    } lr;
+
+    void learn_release()
+    {
+        Buf<float>* fb[] = {&lr.A, &lr.B, &lr.Pw, &lr.Pp, &lr.w, &lr.m1, &lr.m2, &lr.partial};
+        for (auto* b : fb) b->release();
+        lr.GL.release(); lr.dw.release(); lr.du.release(); lr.fk.release();
+        lr.lpart.release(); lr.loss.release();
+    }
+
+    LearnFeat learn_feat() const
+    {
+        return LearnFeat{kx.p, ky.p, kz.p, lr.Pw.p, lr.Pp.p, c.m2, c.m3, lr.N, lr.lB, lr.salt};
+    }
+
+    void set_dt(double dt) override
+    {
+        if (!(dt > 0.0)) throw std::runtime_error("ftsp_set_dt: dt must be positive");
+        c.dt = dt;
+    }
+
+    void learn_configure(const ftsp_learn_config& cf) override
+    {
+        if (c.scheme != FTSP_SCHEME_SI || !si_G.p) throw std::runtime_error("the learned preconditioner needs the semi-implicit scheme");
+        const int nf = c.nm + 1;
+        if (nf > mlp::NOUT_MAX) throw std::runtime_error("the learned preconditioner supports at most 3 interaction modes");
+        learn_release();
+        lr = Learn{};
+        lr.nout = nf;
+        lr.np = mlp::n_params(nf);
+        lr.N = (float)cf.N;
+        lr.lB = (float)cf.lB;
+        lr.salt = (float)cf.salt;
+        if (cf.lr > 0.0) lr.lr = cf.lr;
+        if (cf.batch > 0) lr.batch = (cf.batch + mlp::GRAD_THREADS - 1) / mlp::GRAD_THREADS * mlp::GRAD_THREADS;
+        if (cf.refresh_every > 0) lr.refresh_every = cf.refresh_every;
+        if (cf.fallback_ratio > 0.0) lr.fallback = cf.fallback_ratio;
+        lr.seed = cf.seed;
+        lr.nb = lr.batch / mlp::GRAD_THREADS;
+        const size_t Vn = V_;
+        lr.A.alloc(nf * Vn); lr.B.alloc(nf * Vn); lr.Pw.alloc(Vn); lr.Pp.alloc(Vn);
+        lr.GL.alloc(nf * Vn); lr.dw.alloc(nf * Vn); lr.du.alloc(nf * Vn); lr.fk.alloc(2 * Vn);
+        lr.w.alloc(lr.np); lr.m1.alloc(lr.np); lr.m2.alloc(lr.np);
+        lr.partial.alloc((size_t)lr.nb * lr.np); lr.lpart.alloc(2 * (size_t)lr.nb); lr.loss.alloc(2);
+        FTSP_CUDA(cudaMemsetAsync(lr.A.p, 0, sizeof(float) * nf * Vn, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.B.p, 0, sizeof(float) * nf * Vn, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.Pw.p, 0, sizeof(float) * Vn, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.Pp.p, 0, sizeof(float) * Vn, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.m1.p, 0, sizeof(float) * lr.np, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.m2.p, 0, sizeof(float) * lr.np, stream));
+        // Glorot-uniform weights, zero biases, from the configured seed
+        std::vector<float> w(lr.np, 0.0f);
+        uint64_t st = cf.seed * 6364136223846793005ull + 1442695040888963407ull;
+        auto uni = [&st]() {   // 64-bit LCG (Knuth's MMIX constants), top 24 bits
+            st = st * 6364136223846793005ull + 1442695040888963407ull;
+            return (float)((st >> 40) * (1.0 / 16777216.0));
+        };
+        auto fill = [&](int off, int fan_in, int fan_out, int n) {
+            const float a = std::sqrt(6.0f / (float)(fan_in + fan_out));
+            for (int k = 0; k < n; ++k) w[off + k] = (2.0f * uni() - 1.0f) * a;
+        };
+        fill(0, mlp::NIN, mlp::H, mlp::H * mlp::NIN);
+        fill(mlp::off_w2(), mlp::H, mlp::H, mlp::H * mlp::H);
+        fill(mlp::off_w3(), mlp::H, nf, nf * mlp::H);
+        FTSP_CUDA(cudaMemcpyAsync(lr.w.p, w.data(), sizeof(float) * lr.np, cudaMemcpyHostToDevice, stream));
+        FTSP_CUDA(cudaMemcpyAsync(lr.GL.p, si_G.p, sizeof(T) * nf * Vn, cudaMemcpyDeviceToDevice, stream));
+        FTSP_CUDA(cudaMemsetAsync(&ds->lr_use, 0, 3 * sizeof(int), stream));
+        FTSP_CUDA(cudaMemsetAsync(ds->lres_sum, 0, sizeof(ds->lres_sum), stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        lr.configured = true;
+    }
+
+    void learn_require() const
+    {
+        if (!lr.configured) throw std::runtime_error("ftsp_learn_configure has not been called");
+    }
+
+    void learn_collect(bool on) override
+    {
+        learn_require();
+        lr.on_collect = on;
+    }
+
+    // clears the collected (force, increment) statistics and the residual
+    // sums; the network, its optimiser state and the spectral powers are kept
+    void learn_reset() override
+    {
+        learn_require();
+        const size_t n = (size_t)lr.nout * V_;
+        FTSP_CUDA(cudaMemsetAsync(lr.A.p, 0, sizeof(float) * n, stream));
+        FTSP_CUDA(cudaMemsetAsync(lr.B.p, 0, sizeof(float) * n, stream));
+        FTSP_CUDA(cudaMemsetAsync(ds->lres_sum, 0, sizeof(ds->lres_sum), stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        lr.collected = 0;
+    }
+
+    // after the predictor's densities and drifts: the drift change du =
+    // u(omega_bar) - u(omega) in k-space, against the increment dw stashed by
+    // the predictor.  Collects <Re(du dw*)>, <|dw|^2>; while the learned G is
+    // in use, compares the force residuals |du - G dw|^2 of the learned and
+    // the analytic G and selects the kernel of the next step.
+    void learn_after_predictor()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, nf = nm + 1;
+        V* du = lr.du.p;
+        {
+            const V* u0 = drift.p;
+            const V* u1 = drift_bar.p;
+            const V* p0 = dpsi.p;
+            const V* p1 = dpsi_bar.p;
+            const bool elec = c.elec;
+            foreach(Vn, [=] __device__(size_t i) {
+                for (int a = 0; a < nm; ++a) du[(size_t)a * Vn + i] = csub(u1[(size_t)a * Vn + i], u0[(size_t)a * Vn + i]);
+                du[(size_t)nm * Vn + i] = elec ? csub(p1[i], p0[i]) : mkc<V>(T(0), T(0));
+            });
+        }
+        fft3<-1>(du, nf);
+        const V* dw = lr.dw.p;
+        if (lr.on_collect) {
+            float* A = lr.A.p;
+            float* B = lr.B.p;
+            foreach(Vn * nf, [=] __device__(size_t i) {
+                const V a = du[i], b = dw[i];
+                A[i] += (float)((double)a.x * b.x + (double)a.y * b.y);
+                B[i] += (float)((double)b.x * b.x + (double)b.y * b.y);
+            });
+            ++lr.collected;
+        }
+        if (lr.on_use) {
+            const T* GL = lr.GL.p;
+            const T* GA = si_G.p;
+            reduce<2>(Vn * nf, [=] __device__(size_t i, double* acc) {
+                const V a = du[i], b = dw[i];
+                const double gl = (double)GL[i], ga = (double)GA[i];
+                const double rlx = (double)a.x - gl * b.x, rly = (double)a.y - gl * b.y;
+                const double rax = (double)a.x - ga * b.x, ray = (double)a.y - ga * b.y;
+                acc[0] += rlx * rlx + rly * rly;
+                acc[1] += rax * rax + ray * ray;
+            }, ds->lres);
+            DevScal* d = ds;
+            const double ratio = lr.fallback;
+            k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+                const bool ok = isfinite(d->lres[0]) && d->lres[0] <= ratio * d->lres[1];
+                if (isfinite(d->lres[0]) && isfinite(d->lres[1])) {
+                    d->lres_sum[0] += d->lres[0];
+                    d->lres_sum[1] += d->lres[1];
+                }
+                d->lr_checks += 1;
+                if (!ok) d->lr_fallbacks += 1;
+                d->lr_use = ok ? 1 : 0;
+            });
+            ++launches;
+        }
+    }
+
+    // running spectral powers |FFT f|^2 / V of the first mode and of psi
+    // (mean over the first 200 updates, then an exponential average with the
+    // same window)
+    void learn_power()
+    {
+        const size_t Vn = V_;
+        const V* src[2] = {c.nm > 0 ? omega.p : psi.p, psi.p};
+        fft3<-1>(lr.fk.p, 2, src);
+        const V* fk = lr.fk.p;
+        float* Pw = lr.Pw.p;
+        float* Pp = lr.Pp.p;
+        const float alpha = 1.0f / (float)std::min<long long>(lr.power_updates + 1, 200);
+        const float invV = (float)(1.0 / (double)Vn);
+        const bool have_w = c.nm > 0, elec = c.elec;
+        foreach(Vn, [=] __device__(size_t i) {
+            const V a = fk[i], b = fk[Vn + i];
+            const float pa = have_w ? (float)((double)a.x * a.x + (double)a.y * a.y) * invV : 0.0f;
+            const float pb = elec ? (float)((double)b.x * b.x + (double)b.y * b.y) * invV : 0.0f;
+            Pw[i] += alpha * (pa - Pw[i]);
+            Pp[i] += alpha * (pb - Pp[i]);
+        });
+        ++lr.power_updates;
+    }
+
+    // G_L(k) = G_Debye(k) exp(z(k)) over the grid from the current features
+    void learn_refresh()
+    {
+        const size_t Vn = V_;
+        const int nf = lr.nout;
+        T* GL = lr.GL.p;
+        const T* GA = si_G.p;
+        const LearnFeat ft = learn_feat();
+        auto out = [=] __device__(size_t i, const float* z) {
+            for (int f = 0; f < nf; ++f) {
+                const size_t j = (size_t)f * Vn + i;
+                const T ga = GA[j];
+                // correction factor exp(z) on the analytic coefficient; where
+                // the analytic coefficient vanishes it is kept
+                GL[j] = ga > T(0) ? (T)((double)ga * exp((double)fminf(fmaxf(z[f], -20.0f), 20.0f))) : ga;
+            }
+        };
+        const int blocks = (int)std::min<size_t>((Vn + 127) / 128, 148 * 8);
+        mlp::k_eval<<<blocks, 128, sizeof(float) * lr.np, stream>>>(Vn, lr.w.p, nf, ft, out);
+        ++launches;
+        lr.since_refresh = 0;
+    }
+
+    void learn_after_step()
+    {
+        learn_power();
+        if (lr.on_use && ++lr.since_refresh >= lr.refresh_every) learn_refresh();
+    }
+
+    // Adam on the collected statistics: each iteration draws `batch` wave
+    // vectors (counter-based, from the seed and the iteration), with targets
+    // log(A / (B G_Debye)) per field where A, B and G_Debye are positive.
+    double learn_train(int iterations) override
+    {
+        learn_require();
+        if (lr.collected < 1) throw std::runtime_error("ftsp_learn_train: no statistics collected");
+        const size_t Vn = V_;
+        const int nf = lr.nout;
+        const float* A = lr.A.p;
+        const float* B = lr.B.p;
+        const T* GA = si_G.p;
+        const LearnFeat ft = learn_feat();
+        const uint32_t s0 = (uint32_t)lr.seed, s1 = (uint32_t)(lr.seed >> 32);
+        // target: log of the measured coefficient over the analytic one
+        auto target = [=] __device__(size_t i, int f, float& t, float& m) {
+            const size_t j = (size_t)f * Vn + i;
+            const double a = A[j], b = B[j], ga = (double)GA[j];
+            const bool ok = ga > 0.0 && a > 0.0 && b > 0.0 && isfinite(a) && isfinite(b);
+            t = ok ? (float)log(a / (b * ga)) : 0.0f;
+            m = ok ? 1.0f : 0.0f;
+        };
+        if (!lr.trained) {
+            // output biases start at the mean target of each field
+            double* tsum = reinterpret_cast<double*>(ds->kobs);
+            reduce<2 * mlp::NOUT_MAX>(Vn, [=] __device__(size_t i, double* acc) {
+                for (int f = 0; f < nf; ++f) {
+                    float t, m;
+                    target(i, f, t, m);
+                    acc[2 * f] += (double)(t * m);
+                    acc[2 * f + 1] += (double)m;
+                }
+            }, tsum);
+            double h[2 * mlp::NOUT_MAX];
+            FTSP_CUDA(cudaMemcpyAsync(h, tsum, sizeof(h), cudaMemcpyDeviceToHost, stream));
+            FTSP_CUDA(cudaStreamSynchronize(stream));
+            std::vector<float> b3(nf);
+            for (int f = 0; f < nf; ++f) b3[f] = h[2 * f + 1] > 0.0 ? (float)(h[2 * f] / h[2 * f + 1]) : 0.0f;
+            FTSP_CUDA(cudaMemcpyAsync(lr.w.p + mlp::off_b3(nf), b3.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, stream));
+        }
+        const size_t smem = sizeof(float) * mlp::grad_smem_floats(nf);
+        for (int it = 0; it < iterations; ++it) {
+            const uint32_t iter = (uint32_t)lr.adam_t;
+            auto sample = [=] __device__(int s, float* x, float* t, float* m) {
+                const U4 r = philox(U4{(uint32_t)s, iter, 0x4c45524eu, 0u}, s0, s1);
+                const size_t i = (size_t)((((uint64_t)r.x << 32) | r.y) % (uint64_t)Vn);
+                ft(i, x);
+                for (int f = 0; f < nf; ++f) target(i, f, t[f], m[f]);
+            };
+            auto kern = mlp::k_grad<decltype(sample)>;
+            if (it == 0) set_smem(kern, smem);
+            kern<<<lr.nb, mlp::GRAD_THREADS, smem, stream>>>(lr.batch, lr.w.p, nf, sample, lr.partial.p, lr.lpart.p);
+            mlp::AdamArgs aa{(float)lr.lr, 0.9f, 0.999f, 1e-8f, ++lr.adam_t, 1};
+            mlp::k_reduce_adam<<<(lr.np + 255) / 256, 256, 0, stream>>>(lr.np, lr.nb, lr.partial.p, lr.lpart.p, nullptr,
+                                                                        lr.loss.p, lr.w.p, lr.m1.p, lr.m2.p, aa);
+            launches += 2;
+        }
+        double l[2] = {0.0, 0.0};
+        FTSP_CUDA(cudaMemcpyAsync(l, lr.loss.p, sizeof(l), cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        lr.trained = true;
+        lr.last_loss = l[0];
+        if (lr.on_use) learn_refresh();
+        return l[0];
+    }
+
+    void learn_use(bool on) override
+    {
+        learn_require();
+        if (on && !lr.trained) throw std::runtime_error("ftsp_learn_use: the network has not been trained");
+        lr.on_use = on;
+        const int v = on ? 1 : 0;
+        FTSP_CUDA(cudaMemcpyAsync(&ds->lr_use, &v, sizeof(int), cudaMemcpyHostToDevice, stream));
+        if (on) learn_refresh();
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void learn_stats(ftsp_learn_stats* st) override
+    {
+        pull_scalars();
+        std::memset(st, 0, sizeof(*st));
+        st->collected = lr.collected;
+        st->checks = hs.lr_checks;
+        st->fallbacks = hs.lr_fallbacks;
+        st->residual_learned = hs.lres[0];
+        st->residual_analytic = hs.lres[1];
+        st->residual_learned_sum = hs.lres_sum[0];
+        st->residual_analytic_sum = hs.lres_sum[1];
+        st->loss = lr.last_loss;
+        st->iterations = lr.adam_t;
+        st->using_learned = lr.on_use && hs.lr_use ? 1 : 0;
+        st->n_params = lr.np;
+    }
+
+    int learn_weights(float* out, int n, bool set) override
+    {
+        learn_require();
+        if (!out) return lr.np;
+        if (n != lr.np) throw std::runtime_error("learned weights: expected " + std::to_string(lr.np) + " floats");
+        if (set) {
+            FTSP_CUDA(cudaMemcpyAsync(lr.w.p, out, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+            lr.trained = true;
+            if (lr.on_use) learn_refresh();
+        } else {
+            FTSP_CUDA(cudaMemcpyAsync(out, lr.w.p, sizeof(float) * n, cudaMemcpyDeviceToHost, stream));
+        }
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        return lr.np;
+    }
+
+    // Loss and gradient of the network at the current weights on caller
+    // samples (x: n x 6 features, t and m: n x nout targets and weights),
+    // through the training kernels.
+    double learn_grad(const float* x, const float* t, const float* m, int n, float* grad) override
+    {
+        learn_require();
+        if (n < 1) throw std::runtime_error("learn_grad: no samples");
+        const int nf = lr.nout;
+        Buf<float> dx, dt, dm, part, g;
+        Buf<double> lp, lo;
+        const int nb = (n + mlp::GRAD_THREADS - 1) / mlp::GRAD_THREADS;
+        dx.alloc((size_t)n * mlp::NIN); dt.alloc((size_t)n * nf); dm.alloc((size_t)n * nf);
+        part.alloc((size_t)nb * lr.np); g.alloc(lr.np); lp.alloc(2 * (size_t)nb); lo.alloc(2);
+        FTSP_CUDA(cudaMemcpyAsync(dx.p, x, sizeof(float) * n * mlp::NIN, cudaMemcpyHostToDevice, stream));
+        FTSP_CUDA(cudaMemcpyAsync(dt.p, t, sizeof(float) * n * nf, cudaMemcpyHostToDevice, stream));
+        FTSP_CUDA(cudaMemcpyAsync(dm.p, m, sizeof(float) * n * nf, cudaMemcpyHostToDevice, stream));
+        const float* X = dx.p;
+        const float* Tt = dt.p;
+        const float* Mm = dm.p;
+        auto sample = [=] __device__(int s, float* xx, float* tt, float* mm) {
+            for (int k = 0; k < mlp::NIN; ++k) xx[k] = X[(size_t)s * mlp::NIN + k];
+            for (int f = 0; f < nf; ++f) {
+                tt[f] = Tt[(size_t)s * nf + f];
+                mm[f] = Mm[(size_t)s * nf + f];
+            }
+        };
+        const size_t smem = sizeof(float) * mlp::grad_smem_floats(nf);
+        auto kern = mlp::k_grad<decltype(sample)>;
+        set_smem(kern, smem);
+        kern<<<nb, mlp::GRAD_THREADS, smem, stream>>>(n, lr.w.p, nf, sample, part.p, lp.p);
+        mlp::AdamArgs aa{0.0f, 0.9f, 0.999f, 1e-8f, 1, 0};
+        mlp::k_reduce_adam<<<(lr.np + 255) / 256, 256, 0, stream>>>(lr.np, nb, part.p, lp.p, g.p, lo.p, nullptr, nullptr, nullptr, aa);
+        double l[2];
+        FTSP_CUDA(cudaMemcpyAsync(grad, g.p, sizeof(float) * lr.np, cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaMemcpyAsync(l, lo.p, sizeof(l), cudaMemcpyDeviceToHost, stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        dx.release(); dt.release(); dm.release(); part.release(); g.release(); lp.release(); lo.release();
+        return l[0];
     }
 
     // ---- launch helpers ----
@@ -1409,7 +1844,7 @@ struct Engine : EngineBase {
                 }
                 inc[(size_t)nm * Vn + i] = pv;
             });
-            si_precondition();
+            si_precondition(lr.on_collect || lr.on_use);
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
                 for (int a = 0; a < nm; ++a) ob[(size_t)a * Vn + i] = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
                 const V pv = elec ? cadd(ps[i], inc[(size_t)nm * Vn + i]) : mkc<V>(T(0), T(0));
@@ -1796,11 +2231,42 @@ struct Engine : EngineBase {
         else if (name == "W_type_s") { p = kB.p; n = (size_t)M * Vn; }
         else if (name == "psi_s") { p = kB.p + (size_t)M * Vn; n = Vn; }
         else if (name == "qF") { p = qF.p; n = (size_t)Nmax * Vn; }
-        else if (name == "si_precond" && si_P.p) {
+        else if (name == "si_precond" && si_G.p) {
             const size_t nr = (size_t)(nm + 1) * Vn;
             if (out) {
                 std::vector<T> tmp(nr);
-                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), si_P.p, sizeof(T) * nr, cudaMemcpyDeviceToHost, stream));
+                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), si_G.p, sizeof(T) * nr, cudaMemcpyDeviceToHost, stream));
+                FTSP_CUDA(cudaStreamSynchronize(stream));
+                for (size_t i = 0; i < nr; ++i) {
+                    const size_t f = i / Vn;
+                    const double sf = c.dt * (f < (size_t)nm ? c.lambda[f] : c.lpsi);
+                    out[2 * i] = (double)(T)(1.0 / (1.0 + sf * (double)tmp[i]));
+                    out[2 * i + 1] = 0.0;
+                }
+            }
+            return (long long)(2 * nr);
+        }
+        else if ((name == "learn_A" && lr.A.p) || (name == "learn_B" && lr.B.p) || (name == "learn_Pw" && lr.Pw.p) ||
+                 (name == "learn_Pp" && lr.Pp.p)) {
+            const bool one = name == "learn_Pw" || name == "learn_Pp";
+            const size_t nr = one ? Vn : (size_t)(nm + 1) * Vn;
+            const float* src = name == "learn_A" ? lr.A.p : name == "learn_B" ? lr.B.p : name == "learn_Pw" ? lr.Pw.p : lr.Pp.p;
+            if (out) {
+                std::vector<float> tmp(nr);
+                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * nr, cudaMemcpyDeviceToHost, stream));
+                FTSP_CUDA(cudaStreamSynchronize(stream));
+                for (size_t i = 0; i < nr; ++i) {
+                    out[2 * i] = (double)tmp[i];
+                    out[2 * i + 1] = 0.0;
+                }
+            }
+            return (long long)(2 * nr);
+        }
+        else if ((name == "si_G" && si_G.p) || (name == "learned_G" && lr.GL.p)) {
+            const size_t nr = (size_t)(nm + 1) * Vn;
+            if (out) {
+                std::vector<T> tmp(nr);
+                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), name == "si_G" ? si_G.p : lr.GL.p, sizeof(T) * nr, cudaMemcpyDeviceToHost, stream));
                 FTSP_CUDA(cudaStreamSynchronize(stream));
                 for (size_t i = 0; i < nr; ++i) {
                     out[2 * i] = (double)tmp[i];
@@ -1954,9 +2420,12 @@ struct Engine : EngineBase {
         predictor();
         eval(1, st);
         drifts(1);
+        const bool learn = lr.on_collect || lr.on_use;
+        if (learn) learn_after_predictor();
         kspace_obs();
         finalize_record(st);
         corrector();
+        if (learn) learn_after_step();
         ++step_counter;
         mark_step_status();
         if (c.restart_interval > 0 && step_counter % (uint64_t)c.restart_interval == 0) checkpoint_if_good();

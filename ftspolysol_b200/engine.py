@@ -61,6 +61,18 @@ class ftsp_kernel_stat(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("launches", C.c_longlong), ("bytes", C.c_double)]
 
 
+class ftsp_learn_config(C.Structure):
+    _fields_ = [("N", C.c_double), ("lB", C.c_double), ("salt", C.c_double), ("lr", C.c_double), ("batch", C.c_int),
+                ("refresh_every", C.c_int), ("fallback_ratio", C.c_double), ("seed", C.c_ulonglong)]
+
+
+class ftsp_learn_stats(C.Structure):
+    _fields_ = [("collected", C.c_longlong), ("checks", C.c_longlong), ("fallbacks", C.c_longlong),
+                ("residual_learned", C.c_double), ("residual_analytic", C.c_double),
+                ("residual_learned_sum", C.c_double), ("residual_analytic_sum", C.c_double), ("loss", C.c_double),
+                ("iterations", C.c_int), ("using_learned", C.c_int), ("n_params", C.c_int)]
+
+
 _lib = None
 
 
@@ -103,6 +115,16 @@ def lib():
                                                    vp, C.c_int, C.c_double, vp, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
         L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
+        L.ftsp_set_dt.argtypes = [vp, C.c_double]
+        L.ftsp_learn_configure.argtypes = [vp, C.POINTER(ftsp_learn_config)]
+        L.ftsp_learn_collect.argtypes = [vp, C.c_int]
+        L.ftsp_learn_reset.argtypes = [vp]
+        L.ftsp_learn_train.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
+        L.ftsp_learn_use.argtypes = [vp, C.c_int]
+        L.ftsp_learn_get_stats.argtypes = [vp, C.POINTER(ftsp_learn_stats)]
+        L.ftsp_learn_get_weights.argtypes = [vp, vp, C.POINTER(C.c_int)]
+        L.ftsp_learn_set_weights.argtypes = [vp, vp, C.c_int]
+        L.ftsp_learn_grad.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp]
         _lib = L
     return _lib
 
@@ -112,7 +134,9 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
-               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count")
+               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
+               "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
+               "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad")
 
 
 def _dp(a):
@@ -324,6 +348,58 @@ class Engine:
 
     def set_stream(self, stream_handle: int):
         self._check(lib().ftsp_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    # ---- time step and learned preconditioner (include/ftsp.h) ----
+    def set_dt(self, dt: float):
+        self._check(lib().ftsp_set_dt(self.h, float(dt)), "set_dt")
+
+    def learn_configure(self, N: float, lB: float, salt: float, lr: float = 1e-3, batch: int = 4096,
+                        refresh_every: int = 100, fallback_ratio: float = 1.5, seed: int = 7):
+        cf = ftsp_learn_config(float(N), float(lB), float(salt), float(lr), int(batch), int(refresh_every),
+                               float(fallback_ratio), int(seed))
+        self._check(lib().ftsp_learn_configure(self.h, C.byref(cf)), "learn_configure")
+
+    def learn_collect(self, on: bool = True):
+        self._check(lib().ftsp_learn_collect(self.h, int(bool(on))), "learn_collect")
+
+    def learn_reset(self):
+        self._check(lib().ftsp_learn_reset(self.h), "learn_reset")
+
+    def learn_train(self, iterations: int) -> float:
+        loss = C.c_double()
+        self._check(lib().ftsp_learn_train(self.h, int(iterations), C.byref(loss)), "learn_train")
+        return loss.value
+
+    def learn_use(self, on: bool = True):
+        self._check(lib().ftsp_learn_use(self.h, int(bool(on))), "learn_use")
+
+    def learn_stats(self) -> dict:
+        st = ftsp_learn_stats()
+        self._check(lib().ftsp_learn_get_stats(self.h, C.byref(st)), "learn_get_stats")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def learn_weights(self) -> np.ndarray:
+        n = C.c_int(0)
+        self._check(lib().ftsp_learn_get_weights(self.h, None, C.byref(n)), "learn_get_weights")
+        w = np.zeros(n.value, dtype=np.float32)
+        self._check(lib().ftsp_learn_get_weights(self.h, w.ctypes.data, C.byref(n)), "learn_get_weights")
+        return w
+
+    def learn_set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(lib().ftsp_learn_set_weights(self.h, w.ctypes.data, int(w.size)), "learn_set_weights")
+
+    def learn_grad(self, x: np.ndarray, t: np.ndarray, m: np.ndarray):
+        """(loss, gradient) of the network on caller samples, through the GPU kernels."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        n = x.shape[0]
+        g = np.zeros(self.learn_weights().size, dtype=np.float32)
+        loss = C.c_double()
+        self._check(lib().ftsp_learn_grad(self.h, x.ctypes.data, t.ctypes.data, m.ctypes.data, int(n), C.byref(loss),
+                                          g.ctypes.data), "learn_grad")
+        return loss.value, g
 
     def restarts(self) -> int:
         return int(lib().ftsp_restart_count(self.h))

@@ -172,6 +172,77 @@ int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, d
  * -1 on error.  Synchronises the handle's stream. */
 long long ftsp_restart_count(ftsp_handle* h);
 
+/* Time step of the following steps (the noise amplitude, the predictor and
+ * corrector coefficients and the semi-implicit P(k) follow it).  No
+ * reference counterpart: the reference reads dt once from the param file
+ * (param.cu:228). */
+int ftsp_set_dt(ftsp_handle* h, double dt);
+
+/* Learned semi-implicit preconditioner (no reference counterpart; the
+ * reference has no semi-implicit scheme).  A per-k-mode MLP (features
+ * log(1+k^2), log(1+P_w(k)), log(1+P_psi(k)), N/50, lB, 10*salt; two tanh
+ * layers of width 64; FP32) predicts the linear-response coefficient G_f(k)
+ * = G_f^Debye(k) exp(z_f) of every Langevin field f (interaction modes, then
+ * psi), which replaces the analytic Debye-function G(k) in
+ * P(k) = 1/(1 + lambda dt G(k)).  Handles with scheme FTSP_SCHEME_SI and at
+ * most 3 interaction modes only.
+ *
+ *   ftsp_learn_configure  allocates the statistics and the network (weights
+ *                         from the seed);
+ *   ftsp_learn_collect    while on, every step accumulates, per field and k,
+ *                         <Re(du conj(dw))> and <|dw|^2> of the drift change
+ *                         du = u(omega_bar) - u(omega) and the predictor
+ *                         increment dw (the "force, field-increment" pairs),
+ *                         and the running spectral powers; it may stay on
+ *                         while the learned G(k) is in use (online training);
+ *   ftsp_learn_reset      clears those statistics and the residual sums
+ *                         (network and optimiser kept);
+ *   ftsp_learn_train      runs `iterations` Adam steps (hand-written forward,
+ *                         backward and update kernels) regressing z_f on
+ *                         log(<Re(du dw*)> / (<|dw|^2> G^Debye)); *loss
+ *                         receives the last batch's mean squared error;
+ *   ftsp_learn_use        while on, the SI update uses the learned G(k),
+ *                         re-evaluated every refresh_every steps, except after
+ *                         a step whose force residual sum_k |du - G dw|^2 with
+ *                         the learned G exceeds fallback_ratio times the one
+ *                         with the analytic G: the next step then uses the
+ *                         analytic G (counted in ftsp_learn_stats). */
+typedef struct ftsp_learn_config {
+    double N, lB, salt;          /* system features: chain length, Bjerrum length, salt density */
+    double lr;                   /* Adam step size (<= 0: 1e-3) */
+    int batch;                   /* wave vectors per Adam step, rounded up to 128 (<= 0: 4096) */
+    int refresh_every;           /* steps between re-evaluations of G(k) in use (<= 0: 100) */
+    double fallback_ratio;       /* residual ratio that triggers the analytic kernel (<= 0: 1.5) */
+    unsigned long long seed;     /* weight initialisation and batch sampling */
+} ftsp_learn_config;
+typedef struct ftsp_learn_stats {
+    long long collected;         /* steps whose statistics were accumulated */
+    long long checks, fallbacks; /* steps judged by the residual test; of those, analytic fallbacks */
+    double residual_learned;     /* last step's force residuals */
+    double residual_analytic;
+    double residual_learned_sum; /* their sums over the steps since the last reset */
+    double residual_analytic_sum;
+    double loss;                 /* last training batch loss */
+    int iterations;              /* Adam steps taken */
+    int using_learned;           /* the next step uses the learned G(k) */
+    int n_params;                /* network size in floats */
+} ftsp_learn_stats;
+int ftsp_learn_configure(ftsp_handle* h, const ftsp_learn_config* cfg);
+int ftsp_learn_collect(ftsp_handle* h, int on);
+int ftsp_learn_reset(ftsp_handle* h);
+int ftsp_learn_train(ftsp_handle* h, int iterations, double* loss);
+int ftsp_learn_use(ftsp_handle* h, int on);
+int ftsp_learn_get_stats(ftsp_handle* h, ftsp_learn_stats* stats);
+/* Network weights (layout W1[64][6] b1[64] W2[64][64] b2[64] W3[nout][64]
+ * b3[nout]): get copies them out, set replaces them; *n is the float count
+ * (pass out = NULL to query it). */
+int ftsp_learn_get_weights(ftsp_handle* h, float* out, int* n);
+int ftsp_learn_set_weights(ftsp_handle* h, const float* w, int n);
+/* Loss and its gradient with respect to the weights, through the training
+ * kernels, on caller samples: x [n][6] features, t and m [n][nout] targets and
+ * target weights (loss = sum m (z - t)^2 / sum m).  For gradient checks. */
+int ftsp_learn_grad(ftsp_handle* h, const float* x, const float* t, const float* m, int n, double* loss, float* grad);
+
 /* Device pointers of the resident state (FP64 handles only), in the layout of
  * deviceState (deviceState.h:6-48). */
 typedef struct ftsp_views {
