@@ -49,6 +49,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-line", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--time-to-pi", action="store_true",
+                    help="instead of the throughput line: time for Pi and mu to reach 1%% of the complex128 "
+                         "semi-implicit dt=0.005 result, learned complex64 at dt=0.02 against plain runs")
+    ap.add_argument("--ttp-time", type=float, default=20.0, help="simulated time of each time-to-Pi run")
+    ap.add_argument("--ttp-train-steps", type=int, default=2000,
+                    help="plain semi-implicit steps whose statistics train the network")
     return ap.parse_args()
 
 
@@ -423,6 +429,132 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# time to Pi: learned complex64 SI at dt = 0.02 against the plain runs
+# ---------------------------------------------------------------------------
+def _trajectory(eng, steps, t_wall0, rows, sim0, dt):
+    """Steps with a synchronous record each; rows get (wall s, sim time, Pi, mu)."""
+    import time
+    from ftspolysol_b200.engine import NonFinite
+    bad = 0
+    for k in range(steps):
+        try:
+            _, rec, _ = eng.step()
+            rows.append((time.perf_counter() - t_wall0, sim0 + (k + 1) * dt, rec[-1].real, rec[0].real))
+        except NonFinite:
+            bad += 1   # the device rollback restores the last checkpoint on the next step
+    return bad
+
+
+def _time_to_target(rows, target, tol=0.01, every=50):
+    """Earliest wall time from which on every running estimate (mean of Pi
+    and mu over the second half of the trajectory so far, checked every
+    `every` steps) stays within tol of target."""
+    import numpy as np
+    a = np.array(rows)
+    checks = []
+    for n in range(every, len(a) + 1, every):
+        h = a[n // 2:n]
+        ok = all(abs(h[:, c].mean() - target[i]) <= tol * abs(target[i]) for i, c in enumerate((2, 3)))
+        checks.append((a[n - 1, 0], ok))
+    t_hit = None
+    for t, ok in reversed(checks):
+        if not ok:
+            break
+        t_hit = t
+    return t_hit
+
+
+def run_time_to_pi(args, local):
+    import time
+    import numpy as np
+    import torch
+    from ftspolysol_b200 import Engine, FP32, FP64, SCHEME_SI
+    from ftspolysol_b200.cases import workload
+    from ftspolysol_b200.derive import derive
+
+    torch.cuda.set_device(local)
+    case = workload(5, noise=True)
+    if args.grid != 128:
+        case = scaled_case(case, args.grid)
+    d = derive(case)
+    om, ps = case.initial_fields()
+    T = args.ttp_time
+    salt = case.salt["num_salt"] / case.volume if case.salt else 0.0
+    N = len(case.species[0].monomers)
+    runs = {}
+
+    def plain(prec, dt, tag):
+        e = Engine(dict(d, dt=dt), precision=prec, scheme=SCHEME_SI, noise=True, seed=21, device=local,
+                   restart_interval=20)
+        e.set_fields(om, ps)
+        torch.cuda.synchronize()
+        rows = []
+        t0 = time.perf_counter()
+        bad = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt)
+        runs[tag] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "wall_s": rows[-1][0] if rows else None}
+        e.close()
+
+    plain(FP64, 0.005, "c128_si_dt0.005")
+    half = np.array(runs["c128_si_dt0.005"]["rows"])
+    half = half[len(half) // 2:]
+    target = (float(half[:, 2].mean()), float(half[:, 3].mean()))
+    plain(FP32, 0.005, "c64_si_dt0.005")
+    plain(FP32, 0.02, "c64_si_dt0.02")
+
+    # learned: plain SI steps at dt = 0.005 collect the statistics, Adam trains
+    # the network, then dt = 0.02 with the learned kernel, retrained online
+    e = Engine(dict(d, dt=0.005), precision=FP32, scheme=SCHEME_SI, noise=True, seed=21, device=local, restart_interval=20)
+    e.set_fields(om, ps)
+    e.learn_configure(N=N, lB=case.lB, salt=salt, seed=11)
+    torch.cuda.synchronize()
+    rows = []
+    t0 = time.perf_counter()
+    ntrain = min(args.ttp_train_steps, int(round(T / 0.005)) // 2)
+    e.learn_collect(True)
+    bad = _trajectory(e, ntrain, t0, rows, 0.0, 0.005)
+    loss = e.learn_train(1500)
+    t_train = time.perf_counter() - t0
+    e.set_dt(0.02)
+    e.learn_use(True)
+    e.learn_reset()
+    sim = ntrain * 0.005
+    nbig = int(round((T - sim) / 0.02))
+    done = 0
+    while done < nbig:
+        k = min(200, nbig - done)
+        bad += _trajectory(e, k, t0, rows, sim + done * 0.02, 0.02)
+        done += k
+        e.learn_train(200)
+        e.learn_reset()
+    st = e.learn_stats()
+    runs["c64_learned_dt0.02"] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "wall_s": rows[-1][0],
+                                  "train_steps": ntrain, "train_wall_s": t_train, "train_loss": loss,
+                                  "fallback_steps": st["fallbacks"], "judged_steps": st["checks"]}
+    e.close()
+
+    out = {}
+    for tag, r in runs.items():
+        a = np.array(r["rows"])
+        h = a[len(a) // 2:]
+        info = {k: v for k, v in r.items() if k != "rows"}
+        info.update({"steps": len(a), "Pi_mean": float(h[:, 2].mean()), "mu_mean": float(h[:, 3].mean()),
+                     "Pi_rel_err": float(h[:, 2].mean() / target[0] - 1.0),
+                     "mu_rel_err": float(h[:, 3].mean() / target[1] - 1.0),
+                     "time_to_1pct_s": _time_to_target(r["rows"], target)})
+        out[tag] = info
+    base = out["c128_si_dt0.005"]["time_to_1pct_s"]
+    lt = out["c64_learned_dt0.02"]["time_to_1pct_s"]
+    print(json.dumps({"metric": "time to Pi and mu within 1% of the complex128 semi-implicit dt=0.005 result",
+                      "unit": "s", "higher_is_better": False, "value": lt,
+                      "speedup_vs_c128": (base / lt) if (base and lt) else None,
+                      "target": {"Pi": target[0], "mu_poly_ex": target[1]}, "simulated_time": T,
+                      "config": {"workload": case.name + ": %d^3, L=%gb, N=50, divalent counterions, salt 0.05"
+                                 % (case.m[0], case.L[0])},
+                      "data": "synthetic", "runs": out}))
+    return 0
+
+
 def derived_bytes(case, prec):
     import numpy as np
     return int(np.prod(case.m)) * (8 if prec == 1 else 16)
@@ -434,6 +566,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, ws, rank)
+        elif args.time_to_pi:
+            rc = run_time_to_pi(args, local) if rank == 0 else 0
         else:
             rc = run_ours(args, ws, rank, local)
     finally:

@@ -144,3 +144,4 @@ def test_fallback_rule_counts(trained):
     st = f.learn_stats()
     assert st["checks"] == 10 and st["fallbacks"] == 10 and st["using_learned"] == 0
     f.close()
+
