@@ -55,6 +55,10 @@ def parse_args():
     ap.add_argument("--ttp-time", type=float, default=20.0, help="simulated time of each time-to-Pi run")
     ap.add_argument("--ttp-train-steps", type=int, default=2000,
                     help="plain semi-implicit steps whose statistics train the network")
+    ap.add_argument("--replicas", type=int, default=0,
+                    help="instead of the throughput line: this many independent replicas of uneven grids "
+                         "(32^3-96^3), spread over the ranks and stepped as one CUDA graph per rank")
+    ap.add_argument("--steps-per-graph", type=int, default=2)
     return ap.parse_args()
 
 
@@ -147,8 +151,11 @@ def dist_setup():
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+        else:   # CPU runs of the rank logic (tests)
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
     return ws, rank, local
 
 
@@ -157,8 +164,20 @@ def dist_max(x: float, ws: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -555,6 +574,93 @@ def run_time_to_pi(args, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# replicas: many independent systems of uneven size, one CUDA graph per rank
+# ---------------------------------------------------------------------------
+def run_replicas(args, ws, rank, local):
+    import numpy as np
+    import torch
+    from ftspolysol_b200 import Engine, FP32, SCHEME_SI
+    from ftspolysol_b200.derive import derive
+    from ftspolysol_b200.engine import Batch
+    from ftspolysol_b200 import replicas as R
+
+    torch.cuda.set_device(local)
+    cases_all = R.replica_set(args.replicas)
+    mine = R.assign([R.cost(c) for c in cases_all], ws)[rank]
+    engines = []
+    for i in mine:
+        c = cases_all[i]
+        e = Engine(derive(c), precision=FP32, scheme=SCHEME_SI, noise=True, seed=7000 + i, device=local,
+                   restart_interval=10)
+        om, ps = c.initial_fields()
+        e.set_fields(om, ps)
+        engines.append(e)
+    K = max(1, args.steps // args.steps_per_graph)
+    # the same steps launched one engine after another (no graph, one stream)
+    for e in engines:
+        e.step_async()
+    torch.cuda.synchronize()
+    barrier(ws)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record()
+    for _ in range(K * args.steps_per_graph):
+        for e in engines:
+            e.step_async()
+    a1.record()
+    torch.cuda.synchronize()
+    seq_ms = dist_max(a0.elapsed_time(a1), ws)
+    # one graph per rank: every replica on its own branch
+    batch = Batch(engines, args.steps_per_graph)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    batch.step(max(1, args.warmup // args.steps_per_graph))
+    batch.sync()
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(K)
+    e1.record(stream)
+    batch.sync()
+    ck = clocks.stop()
+    barrier(ws)
+    ms = dist_max(e0.elapsed_time(e1), ws)
+    kernels = batch.launches_per_graph
+    batch.close()
+    results = {}
+    for i, e in zip(mine, engines):
+        st, rec, _ = e.read_status()
+        results[i] = {"status": int(st), "restarts": int(e.restarts()), "Pi": float(rec[-1].real) if len(rec) else None,
+                      "grid": cases_all[i].m[0], "N": len(cases_all[i].species[0].monomers)}
+        e.close()
+    results = R.gather(results, ws)
+    steps_done = dist_sum(len(mine) * K * args.steps_per_graph, ws)
+    if rank == 0:
+        by_grid = {}
+        for r in results.values():
+            g = by_grid.setdefault("%d^3" % r["grid"], {"replicas": 0, "restarts": 0})
+            g["replicas"] += 1
+            g["restarts"] += r["restarts"]
+        print(json.dumps({
+            "metric": "replica CL steps/s (%d independent replicas, 32^3-96^3 grids)" % args.replicas,
+            "value": steps_done / (ms * 1e-3), "unit": "replica-steps/s", "n_gpus": ws,
+            "steps": K * args.steps_per_graph, "warmup": args.warmup, "ms_per_step": ms / (K * args.steps_per_graph),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "%d replicas: grids 32/48/64/96^3 (a quarter each), L = 0.5 b x grid, N from "
+                                   "{20, 32, 50}, salt 0.01-0.5 b^-3, own seeds; complex64 semi-implicit, dt 0.005"
+                                   % args.replicas,
+                       "placement": "longest-processing-time over %d rank(s)" % ws,
+                       "graph": {"steps_per_graph": args.steps_per_graph, "kernels_per_graph_rank0": kernels}},
+            "sequential_value": steps_done / (seq_ms * 1e-3),
+            "graph_speedup": seq_ms / ms,
+            "clocks": ck,
+            "replicas_by_grid": by_grid,
+            "finite_replicas": sum(1 for r in results.values() if r["status"] == 0)}))
+    return 0
+
+
 def derived_bytes(case, prec):
     import numpy as np
     return int(np.prod(case.m)) * (8 if prec == 1 else 16)
@@ -566,6 +672,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, ws, rank)
+        elif args.replicas > 0:
+            rc = run_replicas(args, ws, rank, local)
         elif args.time_to_pi:
             rc = run_time_to_pi(args, local) if rank == 0 else 0
         else:

@@ -355,6 +355,158 @@ long long ftsp_last_launch_count(const ftsp_handle* h)
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Replica batches: the steps of many independent systems captured into one
+// CUDA graph, each system on its own stream branch (fork/join through
+// events), so kernels of different replicas run concurrently and a whole
+// batch step costs one graph launch on the host.
+// ---------------------------------------------------------------------------
+struct ftsp_batch {
+    std::vector<ftsp_handle*> hs;
+    std::vector<cudaStream_t> saved;   // the handles' streams before the batch took them
+    std::vector<cudaStream_t> rs;      // one branch stream per replica
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t main = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int steps_per_graph = 1;
+    int device = 0;
+    long long launches = 0;            // kernels of one graph
+    std::string err;
+
+    void release()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        for (size_t i = 0; i < hs.size() && i < saved.size(); ++i)
+            if (hs[i] && hs[i]->eng) hs[i]->eng->stream = saved[i];
+        for (auto e : ev) cudaEventDestroy(e);
+        for (auto s : rs) cudaStreamDestroy(s);
+        ev.clear();
+        rs.clear();
+        if (fork) cudaEventDestroy(fork);
+        if (main) cudaStreamDestroy(main);
+        fork = nullptr;
+        main = nullptr;
+    }
+};
+
+namespace {
+void batch_check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+}  // namespace
+
+extern "C" {
+
+int ftsp_batch_create(ftsp_handle* const* handles, int n, int steps_per_graph, ftsp_batch** out)
+{
+    if (!out || !handles || n < 1 || steps_per_graph < 1) {
+        g_create_error = "ftsp_batch_create: bad argument";
+        return FTSP_ERROR;
+    }
+    *out = nullptr;
+    auto* b = new ftsp_batch();
+    try {
+        for (int i = 0; i < n; ++i) {
+            if (!handles[i] || !handles[i]->eng) throw std::runtime_error("ftsp_batch_create: null handle");
+            b->hs.push_back(handles[i]);
+        }
+        b->device = b->hs[0]->eng->c.device;
+        for (auto* h : b->hs)
+            if (h->eng->c.device != b->device) throw std::runtime_error("ftsp_batch_create: handles on different devices");
+        b->steps_per_graph = steps_per_graph;
+        batch_check(cudaSetDevice(b->device), "cudaSetDevice");
+        batch_check(cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking), "cudaStreamCreate");
+        batch_check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (int i = 0; i < n; ++i) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            batch_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+            b->rs.push_back(s);
+            batch_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+            b->ev.push_back(e);
+        }
+        // finish whatever the handles queued on their own streams
+        for (auto* h : b->hs) batch_check(cudaStreamSynchronize(h->eng->stream), "cudaStreamSynchronize");
+        for (int i = 0; i < n; ++i) {
+            b->saved.push_back(b->hs[i]->eng->stream);
+            b->hs[i]->eng->stream = b->rs[i];
+        }
+        batch_check(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        try {
+            for (int k = 0; k < steps_per_graph; ++k) {
+                batch_check(cudaEventRecord(b->fork, b->main), "cudaEventRecord");
+                for (int i = 0; i < n; ++i) {
+                    batch_check(cudaStreamWaitEvent(b->rs[i], b->fork, 0), "cudaStreamWaitEvent");
+                    b->hs[i]->eng->step(nullptr, nullptr, nullptr, false);
+                    b->launches += b->hs[i]->eng->launches;
+                    batch_check(cudaEventRecord(b->ev[i], b->rs[i]), "cudaEventRecord");
+                    batch_check(cudaStreamWaitEvent(b->main, b->ev[i], 0), "cudaStreamWaitEvent");
+                }
+            }
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(b->main, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        batch_check(cudaStreamEndCapture(b->main, &b->graph), "cudaStreamEndCapture");
+        batch_check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+        *out = b;
+        return FTSP_OK;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        b->release();
+        delete b;
+        return FTSP_ERROR;
+    }
+}
+
+int ftsp_batch_step(ftsp_batch* b, int launches)
+{
+    if (!b || !b->exec) return FTSP_ERROR;
+    for (int i = 0; i < launches; ++i) {
+        const cudaError_t e = cudaGraphLaunch(b->exec, b->main);
+        if (e != cudaSuccess) {
+            b->err = std::string("cudaGraphLaunch: ") + cudaGetErrorString(e);
+            return FTSP_ERROR;
+        }
+    }
+    return FTSP_OK;
+}
+
+int ftsp_batch_sync(ftsp_batch* b)
+{
+    if (!b) return FTSP_ERROR;
+    const cudaError_t e = cudaStreamSynchronize(b->main);
+    if (e != cudaSuccess) {
+        b->err = std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e);
+        return FTSP_ERROR;
+    }
+    return FTSP_OK;
+}
+
+void* ftsp_batch_stream(ftsp_batch* b) { return b ? static_cast<void*>(b->main) : nullptr; }
+
+long long ftsp_batch_launch_count(const ftsp_batch* b) { return b ? b->launches : -1; }
+
+const char* ftsp_batch_last_error(const ftsp_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+void ftsp_batch_destroy(ftsp_batch* b)
+{
+    if (!b) return;
+    if (b->main) cudaStreamSynchronize(b->main);
+    b->release();
+    delete b;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Chain propagation without any device allocation.
 //
 // For callers that cannot call cudaMalloc: code running while a CUDA stream

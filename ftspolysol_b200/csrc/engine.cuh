@@ -62,6 +62,7 @@ struct DevScal {
     alignas(16) double sconn[12];          // connectivity stress sums over the bond-pass CTAs
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
+    alignas(16) unsigned long long step;   // steps taken: keys the noise, schedules the checkpoints
     alignas(16) double lres[2];            // learned preconditioner: force residuals (learned, analytic) of the step
     alignas(16) double lres_sum[2];        // and their sums since the last statistics reset
     alignas(16) int nonfinite;
@@ -553,7 +554,6 @@ struct Engine : EngineBase {
     DevScal* ds = nullptr;
     DevScal hs{};
     bool noise_injected = false;
-    uint64_t step_counter = 0;
     int Nmax = 1;
 
     explicit Engine(const HostCfg& cfg)
@@ -1791,8 +1791,12 @@ struct Engine : EngineBase {
             SigTab sg{};
             for (int a = 0; a < nm; ++a) sg.s[a] = c.noise ? std::sqrt(2.0 * c.lambda[a] * c.dt / c.dV) : 0.0;
             sg.s[nm] = (c.elec && c.noise) ? std::sqrt(2.0 * c.lpsi * c.dt / c.dV) : 0.0;
-            const uint64_t seed = c.seed, st = step_counter;
+            // the step index is read on the device, so a captured step replays
+            // with fresh noise
+            const uint64_t seed = c.seed;
+            const DevScal* d = ds;
             foreach(Vn, [=] __device__(size_t i) {
+                const uint64_t st = d->step;
                 for (int f = 0; f <= nm; ++f)
                     e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)(sg.s[f] * normal_at(seed, st, (uint32_t)f, i)) : T(0);
             });
@@ -2380,10 +2384,13 @@ struct Engine : EngineBase {
             for (int s = 0; s < S; ++s) bad |= !(isfinite(d->Q[s].x) && isfinite(d->Q[s].y));
             for (int i = 0; i < 2 * R; ++i) bad |= !isfinite(d->rec[i]);
             d->bad_last = bad ? 1 : 0;
+            d->step += 1;
         });
         ++launches;
     }
 
+    // copies (omega, psi) to the device checkpoint after every
+    // restart_interval-th finite step; the schedule is decided on the device
     void checkpoint_if_good()
     {
         const size_t Vn = V_;
@@ -2392,8 +2399,9 @@ struct Engine : EngineBase {
         const V* ps = psi.p;
         V* ckp = ck.p;
         const DevScal* d = ds;
+        const unsigned long long every = (unsigned long long)c.restart_interval;
         foreach(Vn, [=] __device__(size_t i) {
-            if (d->bad_last) return;
+            if (d->bad_last || d->step % every != 0) return;
             for (int a = 0; a < nm; ++a) ckp[(size_t)a * Vn + i] = om[(size_t)a * Vn + i];
             ckp[(size_t)nm * Vn + i] = ps[i];
         });
@@ -2426,9 +2434,8 @@ struct Engine : EngineBase {
         finalize_record(st);
         corrector();
         if (learn) learn_after_step();
-        ++step_counter;
         mark_step_status();
-        if (c.restart_interval > 0 && step_counter % (uint64_t)c.restart_interval == 0) checkpoint_if_good();
+        if (c.restart_interval > 0) checkpoint_if_good();
     }
 
     int status_from_host()

@@ -125,6 +125,17 @@ def lib():
         L.ftsp_learn_get_weights.argtypes = [vp, vp, C.POINTER(C.c_int)]
         L.ftsp_learn_set_weights.argtypes = [vp, vp, C.c_int]
         L.ftsp_learn_grad.argtypes = [vp, vp, vp, vp, C.c_int, C.POINTER(C.c_double), vp]
+        L.ftsp_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, C.POINTER(vp)]
+        L.ftsp_batch_step.argtypes = [vp, C.c_int]
+        L.ftsp_batch_sync.argtypes = [vp]
+        L.ftsp_batch_stream.restype = vp
+        L.ftsp_batch_stream.argtypes = [vp]
+        L.ftsp_batch_launch_count.restype = C.c_longlong
+        L.ftsp_batch_launch_count.argtypes = [vp]
+        L.ftsp_batch_last_error.restype = C.c_char_p
+        L.ftsp_batch_last_error.argtypes = [vp]
+        L.ftsp_batch_destroy.restype = None
+        L.ftsp_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -136,7 +147,9 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
                "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
-               "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad")
+               "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad",
+               "ftsp_batch_create", "ftsp_batch_step", "ftsp_batch_sync", "ftsp_batch_stream",
+               "ftsp_batch_launch_count", "ftsp_batch_last_error", "ftsp_batch_destroy")
 
 
 def _dp(a):
@@ -411,3 +424,39 @@ class Engine:
         v = ftsp_views()
         self._check(lib().ftsp_state_views(self.h, C.byref(v)), "state_views")
         return v
+
+
+class Batch:
+    """Independent replicas stepped together: `steps_per_graph` steps of every
+    engine captured into one CUDA graph (one branch stream per engine), one
+    graph launch per `step` call.  The engines must outlive the batch and are
+    not stepped on their own while it exists."""
+
+    def __init__(self, engines, steps_per_graph: int = 1):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
+        h = C.c_void_p()
+        if lib().ftsp_batch_create(arr, len(self.engines), int(steps_per_graph), C.byref(h)) != FTSP_OK:
+            raise FtspError("ftsp_batch_create: " + (lib().ftsp_batch_last_error(None) or b"").decode())
+        self.h = h
+        self.steps_per_graph = int(steps_per_graph)
+        self.launches_per_graph = int(lib().ftsp_batch_launch_count(self.h))
+
+    def stream(self) -> int:
+        return int(lib().ftsp_batch_stream(self.h) or 0)
+
+    def step(self, graph_launches: int = 1):
+        if lib().ftsp_batch_step(self.h, int(graph_launches)) != FTSP_OK:
+            raise FtspError("ftsp_batch_step: " + (lib().ftsp_batch_last_error(self.h) or b"").decode())
+
+    def sync(self):
+        if lib().ftsp_batch_sync(self.h) != FTSP_OK:
+            raise FtspError("ftsp_batch_sync: " + (lib().ftsp_batch_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ftsp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -243,6 +243,26 @@ int ftsp_learn_set_weights(ftsp_handle* h, const float* w, int n);
  * target weights (loss = sum m (z - t)^2 / sum m).  For gradient checks. */
 int ftsp_learn_grad(ftsp_handle* h, const float* x, const float* t, const float* m, int n, double* loss, float* grad);
 
+/* Replica batches (no reference counterpart: the reference runs one system
+ * per process).  ftsp_batch_create captures steps_per_graph steps of every
+ * handle into one CUDA graph, each handle on its own branch stream, so the
+ * kernels of independent replicas run concurrently and a batch step is one
+ * graph launch.  The handles keep their state and can be read with
+ * ftsp_read_status / ftsp_get_field after ftsp_batch_sync; they must not be
+ * stepped on their own while the batch exists (they run on the batch's
+ * branch streams until ftsp_batch_destroy gives them back their streams).
+ * The noise index and the checkpoint schedule advance on the device, so
+ * every replay takes fresh noise.  Settings that the step reads on the host
+ * (dt, the learned-preconditioner mode) are fixed at capture time. */
+typedef struct ftsp_batch ftsp_batch;
+int ftsp_batch_create(ftsp_handle* const* handles, int n, int steps_per_graph, ftsp_batch** out);
+int ftsp_batch_step(ftsp_batch* b, int graph_launches);       /* asynchronous */
+int ftsp_batch_sync(ftsp_batch* b);
+void* ftsp_batch_stream(ftsp_batch* b);                       /* the stream the graph runs on */
+long long ftsp_batch_launch_count(const ftsp_batch* b);       /* kernels per graph launch */
+const char* ftsp_batch_last_error(const ftsp_batch* b);       /* NULL: errors of ftsp_batch_create */
+void ftsp_batch_destroy(ftsp_batch* b);
+
 /* Device pointers of the resident state (FP64 handles only), in the layout of
  * deviceState (deviceState.h:6-48). */
 typedef struct ftsp_views {
