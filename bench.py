@@ -592,7 +592,7 @@ def run_replicas(args, ws, rank, local):
     for i in mine:
         c = cases_all[i]
         e = Engine(derive(c), precision=FP32, scheme=SCHEME_SI, noise=True, seed=7000 + i, device=local,
-                   restart_interval=10)
+                   restart_interval=10, autotune=True)
         om, ps = c.initial_fields()
         e.set_fields(om, ps)
         engines.append(e)
@@ -629,6 +629,14 @@ def run_replicas(args, ws, rank, local):
     ms = dist_max(e0.elapsed_time(e1), ws)
     kernels = batch.launches_per_graph
     batch.close()
+    tuned = {}
+    for i, e in zip(mine, engines):
+        t = e.tune_info()
+        key = "%d^3" % cases_all[i].m[0]
+        if key not in tuned or t["tuned"]:
+            tuned[key] = {"compile_time_kernels": bool(t["compile_time"]), "max_radix": t["max_radix"],
+                          "tile_width": t["tile_width"], "candidates": t["candidates"],
+                          "fft_pair_ms": t["best_ms"], "default_fft_pair_ms": t["default_ms"]}
     results = {}
     for i, e in zip(mine, engines):
         st, rec, _ = e.read_status()
@@ -652,7 +660,8 @@ def run_replicas(args, ws, rank, local):
                                    "{20, 32, 50}, salt 0.01-0.5 b^-3, own seeds; complex64 semi-implicit, dt 0.005"
                                    % args.replicas,
                        "placement": "longest-processing-time over %d rank(s)" % ws,
-                       "graph": {"steps_per_graph": args.steps_per_graph, "kernels_per_graph_rank0": kernels}},
+                       "graph": {"steps_per_graph": args.steps_per_graph, "kernels_per_graph_rank0": kernels},
+                       "autotune_rank0": tuned},
             "sequential_value": steps_done / (seq_ms * 1e-3),
             "graph_speedup": seq_ms / ms,
             "clocks": ck,

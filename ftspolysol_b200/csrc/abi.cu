@@ -75,6 +75,7 @@ HostCfg make_cfg(const ftsp_config* in)
     c.scheme = in->scheme;
     c.device = in->device;
     c.restart_interval = in->restart_interval > 0 ? in->restart_interval : 0;
+    c.autotune = in->autotune != 0 ? 1 : 0;
     if (c.record_len() > 128) throw std::runtime_error("observable record too long");
     return c;
 }
@@ -222,6 +223,13 @@ int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max)
     int st = FTSP_ERROR;
     FTSP_GUARD(h, st = h->eng->read_status(record, drift_max));
     return st;
+}
+
+int ftsp_tune_info_get(ftsp_handle* h, ftsp_tune_info* info)
+{
+    if (!info) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->tune_info(info));
+    return FTSP_OK;
 }
 
 int ftsp_set_dt(ftsp_handle* h, double dt)

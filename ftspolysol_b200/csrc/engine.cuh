@@ -16,7 +16,10 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -112,6 +115,7 @@ struct HostCfg {
     uint64_t seed;
     int precision, scheme, device;
     int restart_interval;   // device checkpoint every so many steps; rollback on a non-finite step (0: off)
+    int autotune;           // time the launch-geometry alternatives at creation
     int n_stress() const { return __builtin_popcount(stress_mask); }
     bool stress_on() const { return stress_mask != 0 || iso; }
     int record_len() const
@@ -487,6 +491,7 @@ struct EngineBase {
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
     virtual long long restarts() = 0;
     virtual void set_dt(double dt) = 0;
+    virtual void tune_info(ftsp_tune_info* t) = 0;
     virtual void learn_configure(const ftsp_learn_config& cf) = 0;
     virtual void learn_collect(bool on) = 0;
     virtual void learn_reset() = 0;
@@ -564,6 +569,7 @@ struct Engine : EngineBase {
         setup_geometry();
         allocate();
         build_tables();
+        if (c.autotune) autotune();
     }
 
     ~Engine() override
@@ -597,15 +603,25 @@ struct Engine : EngineBase {
         if (bytes > 48 * 1024) FTSP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     }
 
-    void setup_geometry()
+    // Launch geometry of the runtime-plan passes.  max_bits: largest
+    // power-of-two radix (as a bit count) of the FFT plans (0: the default,
+    // 4 for complex64 and 3 for complex128); W: z-columns per tile of the
+    // strided line passes (0: the largest divisor of m3 within the register
+    // budget).  The autotuner times the alternatives (autotune()).
+    int geo_max_bits = 0, geo_W = 0;
+    static int default_max_bits() { return F32 ? 4 : 3; }
+    int w_max() const { return std::max(1, std::min(sizeof(T) == 4 ? 32 : 16, (EL * 256) / std::max(c.m1, c.m2))); }
+
+    void setup_geometry(int max_bits = 0, int Wsel = 0)
     {
         const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
         int dev_smem = 0;
         FTSP_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
         pg.m1 = m1; pg.m2 = m2; pg.m3 = m3; pg.P = m3 + 1;
-        const int max_bits = F32 ? 4 : 3;
+        if (max_bits <= 0) max_bits = default_max_bits();
+        geo_max_bits = max_bits;
         const FftPlan1 hp[3] = {make_plan(m1, max_bits), make_plan(m2, max_bits), make_plan(m3, max_bits)};
-        plans.alloc(3);
+        if (!plans.p) plans.alloc(3);
         FTSP_CUDA(cudaMemcpy(plans.p, hp, sizeof(hp), cudaMemcpyHostToDevice));
         pg.py = plans.p + 1;
         pg.pz = plans.p + 2;
@@ -615,8 +631,9 @@ struct Engine : EngineBase {
         plane_smem = std::max(plane_smem, (size_t)32 * 16 * 8);
         plane_threads = round32((m2 * m3 + EP - 1) / EP);
         plane_ok = plane_smem <= (size_t)dev_smem && plane_threads <= 512;
-        const int wmax = std::max(1, std::min(sizeof(T) == 4 ? 32 : 16, (EL * 256) / std::max(m1, m2)));
-        const int W = pick_W(m3, wmax);
+        const int wmax = w_max();
+        const int W = (Wsel > 0 && Wsel <= wmax && m3 % Wsel == 0) ? Wsel : pick_W(m3, wmax);
+        geo_W = W;
         gx = LineGeom{m1, m2, m3, m1, W, 0, W, plans.p + 0, make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
         gy = LineGeom{m1, m2, m3, m2, W, 0, W, plans.p + 1, make_fastdiv(W), make_fastdiv(1), make_fastdiv(m2), make_fastdiv(m3)};
         x_threads = round32((m1 * W + EL - 1) / EL);
@@ -668,6 +685,111 @@ struct Engine : EngineBase {
         FTSP_CUDA(cudaMemset(omega.p, 0, sizeof(V) * nmv));
         FTSP_CUDA(cudaMemset(psi.p, 0, sizeof(V) * Vn));
         FTSP_CUDA(cudaMemset(eta.p, 0, sizeof(T) * eta.n));
+    }
+
+    // ---- autotuner ----
+    // For every candidate geometry (FFT radix cap, strided tile width) the
+    // forward and inverse 3-D transforms of one field are timed with CUDA
+    // events (one warm-up, then the mean of three); the fastest is kept.
+    // Results are cached per (grid, precision, device) for the process, so a
+    // set of replicas of the same grid tunes once.  Grids whose passes are
+    // all compile-time kernels (32/64/128 cubes) have nothing to tune.
+    struct TuneKey {
+        int m1, m2, m3, f32, dev;
+        bool operator<(const TuneKey& o) const
+        {
+            return std::tie(m1, m2, m3, f32, dev) < std::tie(o.m1, o.m2, o.m3, o.f32, o.dev);
+        }
+    };
+    struct TuneResult {
+        int max_bits = 0, W = 0, candidates = 0;
+        double best_ms = 0.0, default_ms = 0.0;
+        bool tuned = false, cached = false;
+    };
+    static std::map<TuneKey, TuneResult>& tune_cache()
+    {
+        static std::map<TuneKey, TuneResult> m;
+        return m;
+    }
+    static std::mutex& tune_mutex()
+    {
+        static std::mutex m;
+        return m;
+    }
+    TuneResult tune{};
+
+    bool all_compile_time() const
+    {
+        const bool plane = plane_ok && c.m2 == c.m3 && (c.m3 == 32 || c.m3 == 64 || c.m3 == 128) &&
+                           (F32 || c.m3 != 128);
+        return plane && strided_is_ct(c.m1);
+    }
+
+    double time_fft(int reps)
+    {
+        cudaEvent_t a, b;
+        FTSP_CUDA(cudaEventCreate(&a));
+        FTSP_CUDA(cudaEventCreate(&b));
+        fft3<-1>(G.p, 1);
+        fft3<+1>(G.p, 1);
+        FTSP_CUDA(cudaEventRecord(a, stream));
+        for (int r = 0; r < reps; ++r) {
+            fft3<-1>(G.p, 1);
+            fft3<+1>(G.p, 1);
+        }
+        FTSP_CUDA(cudaEventRecord(b, stream));
+        FTSP_CUDA(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        FTSP_CUDA(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return (double)ms / reps;
+    }
+
+    void autotune()
+    {
+        const TuneKey key{c.m1, c.m2, c.m3, F32 ? 1 : 0, c.device};
+        std::lock_guard<std::mutex> lock(tune_mutex());
+        auto it = tune_cache().find(key);
+        if (it != tune_cache().end()) {
+            tune = it->second;
+            tune.cached = true;
+            setup_geometry(tune.max_bits, tune.W);
+            return;
+        }
+        TuneResult r{};
+        if (all_compile_time()) {
+            r.max_bits = geo_max_bits;
+            r.W = geo_W;
+            tune_cache()[key] = r;
+            tune = r;
+            return;
+        }
+        FTSP_CUDA(cudaMemsetAsync(G.p, 0, sizeof(V) * V_, stream));
+        std::vector<int> bits = F32 ? std::vector<int>{2, 3, 4} : std::vector<int>{2, 3};
+        std::vector<int> Ws;
+        for (int w = w_max(); w >= 1 && Ws.size() < 3; --w)
+            if (c.m3 % w == 0) Ws.push_back(w);
+        setup_geometry(0, 0);
+        r.default_ms = time_fft(3);
+        r.best_ms = r.default_ms;
+        r.max_bits = geo_max_bits;
+        r.W = geo_W;
+        for (int mb : bits)
+            for (int w : Ws) {
+                setup_geometry(mb, w);
+                const double t = time_fft(3);
+                ++r.candidates;
+                if (t < r.best_ms) {
+                    r.best_ms = t;
+                    r.max_bits = mb;
+                    r.W = w;
+                }
+            }
+        setup_geometry(r.max_bits, r.W);
+        r.tuned = true;
+        tune_cache()[key] = r;
+        tune = r;
     }
 
     template <typename X>
@@ -898,6 +1020,19 @@ struct Engine : EngineBase {
     LearnFeat learn_feat() const
     {
         return LearnFeat{kx.p, ky.p, kz.p, lr.Pw.p, lr.Pp.p, c.m2, c.m3, lr.N, lr.lB, lr.salt};
+    }
+
+    void tune_info(ftsp_tune_info* t) override
+    {
+        std::memset(t, 0, sizeof(*t));
+        t->tuned = tune.tuned ? 1 : 0;
+        t->cached = tune.cached ? 1 : 0;
+        t->compile_time = all_compile_time() ? 1 : 0;
+        t->max_radix = 1 << geo_max_bits;
+        t->tile_width = geo_W;
+        t->candidates = tune.candidates;
+        t->best_ms = tune.best_ms;
+        t->default_ms = tune.default_ms;
     }
 
     void set_dt(double dt) override

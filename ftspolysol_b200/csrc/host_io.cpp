@@ -419,7 +419,7 @@ void usage(const char* program)
 {
     std::fprintf(stderr,
                  "usage: %s [-p param] [-i id] [-s dir] [--omega omega_file] [--psi psi_file] [--seq sequence_file] "
-                 "[--screenprint] [--fp32|--fp64] [--si|--pc] [--seed N] [--device N]\n",
+                 "[--screenprint] [--fp32|--fp64] [--si|--pc] [--seed N] [--device N] [--autotune]\n",
                  program);
 }
 
@@ -464,6 +464,8 @@ int parse_args(int argc, char** argv, Options& o, std::string& err)
             o.precision = FTSP_FP32;
         } else if (a == "--fp64") {
             o.precision = FTSP_FP64;
+        } else if (a == "--autotune") {
+            o.autotune = 1;
         } else if (a == "--si") {
             o.scheme = FTSP_SCHEME_SI;
         } else if (a == "--pc") {

@@ -45,7 +45,7 @@ struct Options {
     bool omega_override = false, psi_override = false, sequence_override = false;
     bool run_id_set = false, run_parent_set = false, screenprint = false;
     // engine options (no reference counterpart)
-    int precision = 0, scheme = 0, device = 0;
+    int precision = 0, scheme = 0, device = 0, autotune = 0;
     bool seed_set = false;
     unsigned long long seed = 0;
 };

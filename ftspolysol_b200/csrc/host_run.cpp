@@ -520,6 +520,7 @@ int run_main(int argc, char** argv)
     cfg.scheme = o.scheme;
     cfg.device = o.device;
     cfg.restart_interval = 0;
+    cfg.autotune = o.autotune;
     if (o.seed_set) cfg.seed = o.seed;
     else {
         // a fresh seed per run, like the reference's clock-derived curand seeds

@@ -47,7 +47,7 @@ class ftsp_config(C.Structure):
         ("ion_smear", C.POINTER(C.c_double)),
         ("self_pressure", C.c_double), ("stress_mask", C.c_int), ("isotropic_pressure", C.c_int),
         ("noise", C.c_int), ("seed", C.c_ulonglong), ("precision", C.c_int), ("scheme", C.c_int),
-        ("device", C.c_int), ("restart_interval", C.c_int),
+        ("device", C.c_int), ("restart_interval", C.c_int), ("autotune", C.c_int),
     ]
 
 
@@ -59,6 +59,11 @@ class ftsp_views(C.Structure):
 
 class ftsp_kernel_stat(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("launches", C.c_longlong), ("bytes", C.c_double)]
+
+
+class ftsp_tune_info(C.Structure):
+    _fields_ = [("tuned", C.c_int), ("cached", C.c_int), ("compile_time", C.c_int), ("max_radix", C.c_int),
+                ("tile_width", C.c_int), ("candidates", C.c_int), ("best_ms", C.c_double), ("default_ms", C.c_double)]
 
 
 class ftsp_learn_config(C.Structure):
@@ -116,6 +121,7 @@ def lib():
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
         L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
         L.ftsp_set_dt.argtypes = [vp, C.c_double]
+        L.ftsp_tune_info_get.argtypes = [vp, C.POINTER(ftsp_tune_info)]
         L.ftsp_learn_configure.argtypes = [vp, C.POINTER(ftsp_learn_config)]
         L.ftsp_learn_collect.argtypes = [vp, C.c_int]
         L.ftsp_learn_reset.argtypes = [vp]
@@ -146,6 +152,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
                "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
+               "ftsp_tune_info_get",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
                "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad",
                "ftsp_batch_create", "ftsp_batch_step", "ftsp_batch_sync", "ftsp_batch_stream",
@@ -193,7 +200,7 @@ class Engine:
     """
 
     def __init__(self, derived: dict, precision: int = FP64, scheme: int = SCHEME_PC, noise: bool = False,
-                 seed: int = 0, device: int = 0, restart_interval: int = 0):
+                 seed: int = 0, device: int = 0, restart_interval: int = 0, autotune: bool = False):
         L = lib()
         self._keep = []
 
@@ -253,6 +260,7 @@ class Engine:
         cfg.scheme = int(scheme)
         cfg.device = int(device)
         cfg.restart_interval = int(restart_interval)
+        cfg.autotune = int(bool(autotune))
         self.precision = precision
         self._cfg = cfg
         h = C.c_void_p()
@@ -361,6 +369,11 @@ class Engine:
 
     def set_stream(self, stream_handle: int):
         self._check(lib().ftsp_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def tune_info(self) -> dict:
+        t = ftsp_tune_info()
+        self._check(lib().ftsp_tune_info_get(self.h, C.byref(t)), "tune_info")
+        return {k: getattr(t, k) for k, _ in t._fields_}
 
     # ---- time step and learned preconditioner (include/ftsp.h) ----
     def set_dt(self, dt: float):

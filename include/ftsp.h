@@ -81,6 +81,9 @@ typedef struct ftsp_config {
                                     rollback after a non-finite step (the
                                     reference's Ntmp / max_nan_restarts recovery,
                                     complexLangevin.cu:583-636); 0: off          */
+    int autotune;                /* 1: time the launch-geometry alternatives of the
+                                    runtime-plan passes at creation (cached per
+                                    grid in the process); no reference counterpart */
 } ftsp_config;
 
 typedef struct ftsp_handle ftsp_handle;
@@ -242,6 +245,18 @@ int ftsp_learn_set_weights(ftsp_handle* h, const float* w, int n);
  * kernels, on caller samples: x [n][6] features, t and m [n][nout] targets and
  * target weights (loss = sum m (z - t)^2 / sum m).  For gradient checks. */
 int ftsp_learn_grad(ftsp_handle* h, const float* x, const float* t, const float* m, int n, double* loss, float* grad);
+
+/* Launch geometry chosen for the handle's grid (autotune = 1): FFT radix
+ * cap, strided tile width, how many alternatives were timed and the time of
+ * one forward + inverse 3-D transform with the chosen and with the default
+ * geometry.  compile_time = 1: every pass of this grid is a compile-time
+ * kernel and nothing was tuned.  No reference counterpart. */
+typedef struct ftsp_tune_info {
+    int tuned, cached, compile_time;
+    int max_radix, tile_width, candidates;
+    double best_ms, default_ms;
+} ftsp_tune_info;
+int ftsp_tune_info_get(ftsp_handle* h, ftsp_tune_info* info);
 
 /* Replica batches (no reference counterpart: the reference runs one system
  * per process).  ftsp_batch_create captures steps_per_graph steps of every

@@ -76,3 +76,30 @@ def test_replays_draw_fresh_noise():
     assert not np.array_equal(w1, w2)
     e.close()
     ref.close()
+
+
+def test_autotuner_picks_a_geometry_and_keeps_results():
+    """48^3 runs the runtime-plan passes: the tuner times the alternatives,
+    keeps the fastest, caches it for the next handle of the same grid, and
+    the step agrees with the default geometry to round-off (complex128)."""
+    c = small((48, 48, 48), 8, 5)
+    d = derive(c)
+    om, ps = c.initial_fields()
+    eta = np.random.default_rng(2).standard_normal((2, c.size)) * 0.1
+    runs = []
+    for tune in (False, True, True):
+        e = Engine(d, precision=FP64, scheme=SCHEME_PC, autotune=tune)
+        e.set_fields(om, ps)
+        e.step(eta)
+        runs.append((e.tune_info(), e.get("omega"), e.get("rho_type")))
+        e.close()
+    t0, t1, t2 = (r[0] for r in runs)
+    assert t0["tuned"] == 0 and t1["tuned"] == 1 and t1["candidates"] >= 3
+    assert t1["best_ms"] <= t1["default_ms"]
+    assert t2["cached"] == 1 and (t2["max_radix"], t2["tile_width"]) == (t1["max_radix"], t1["tile_width"])
+    for r in runs[1:]:
+        for a, b in zip(r[1:], runs[0][1:]):
+            assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(b))
+    e = Engine(derive(small((32, 32, 32), 8, 6)), precision=FP32, scheme=SCHEME_SI, autotune=True)
+    assert e.tune_info()["compile_time"] == 1
+    e.close()
