@@ -569,6 +569,7 @@ struct Engine : EngineBase {
         setup_geometry();
         allocate();
         build_tables();
+        plan_charge_fold();
         if (c.autotune) autotune();
     }
 
@@ -1644,7 +1645,12 @@ struct Engine : EngineBase {
         }
         // ---- backward sweep (opposite sign convention: B' = B(-k)) ----
         auto rho_of = [&](int seg) { return dB.p + (size_t)s.type[seg] * Vn; };
-        auto rchg = [&](int seg) -> V* { return (c.elec && s.charge[seg] != 0.0) ? dB.p + (size_t)M * Vn : nullptr; };
+        // species whose charge density folds into its type channel after the
+        // sweep (charge_fold) accumulate no separate charge density
+        const bool folded = fold_type[isp] >= 0;
+        auto rchg = [&](int seg) -> V* {
+            return (c.elec && s.charge[seg] != 0.0 && !folded) ? dB.p + (size_t)M * Vn : nullptr;
+        };
         if (N == 1) {
             OpProp<T, BWD_SINGLE> op{};
             op.qread = qf(0); op.rho_type = rho_of(0); op.rho_charge = rchg(0); op.z = (T)s.charge[0]; op.factor = factor;
@@ -1700,6 +1706,61 @@ struct Engine : EngineBase {
         ob.phiz = base + c.m1 + c.m2;
         ob.kx = kx.p; ob.ky = ky.p; ob.kz = kz.p;
         ob.invV = (T)(1.0 / (double)V_);
+    }
+
+    // ---- charge densities of single-class species ----
+    // A species whose segments all share one type t and one valence z, and
+    // which is the only species with segments of type t, has the charge
+    // density z rho_t of its type channel.  Its backward sweep then skips the
+    // read-modify-write of the charge accumulator (two of the eight complex
+    // values per point that the backward segment pass moves), and one pass
+    // after all sweeps adds z rho_t to the charge channel.  For z = +-1, +-2
+    // (powers of two) the result is bit-identical to accumulating it.
+    std::vector<int> fold_type;
+    std::vector<double> fold_z;
+
+    void plan_charge_fold()
+    {
+        const int S = (int)c.sp.size();
+        fold_type.assign(S, -1);
+        fold_z.assign(S, 0.0);
+        if (!c.elec) return;
+        std::vector<int> users(c.M, 0);
+        for (const auto& sp : c.sp) {
+            std::vector<int> seen(c.M, 0);
+            for (int t : sp.type) seen[t] = 1;
+            for (int t = 0; t < c.M; ++t) users[t] += seen[t];
+        }
+        for (int k = 0; k < S; ++k) {
+            const auto& sp = c.sp[k];
+            bool one = true;
+            for (int i = 1; i < sp.N; ++i) one &= sp.type[i] == sp.type[0] && sp.charge[i] == sp.charge[0];
+            if (one && sp.charge[0] != 0.0 && users[sp.type[0]] == 1) {
+                fold_type[k] = sp.type[0];
+                fold_z[k] = sp.charge[0];
+            }
+        }
+    }
+
+    void charge_fold()
+    {
+        ClsTab ft{};
+        int n = 0;
+        for (size_t k = 0; k < fold_type.size(); ++k)
+            if (fold_type[k] >= 0 && n < 32) {
+                ft.type[n] = fold_type[k];
+                ft.z[n] = fold_z[k];
+                ++n;
+            }
+        if (n == 0) return;
+        const size_t Vn = V_;
+        V* dBp = dB.p;
+        const int M = c.M;
+        foreach(Vn, [=] __device__(size_t i) {
+            V acc = dBp[(size_t)M * Vn + i];
+            for (int k = 0; k < n; ++k) acc = cadd(acc, cscale(dBp[(size_t)ft.type[k] * Vn + i], (T)ft.z[k]));
+            dBp[(size_t)M * Vn + i] = acc;
+        });
     }
 
     // ---- densities at (omega_w, psi_w) ----
@@ -1787,6 +1848,7 @@ struct Engine : EngineBase {
         if (stress) FTSP_CUDA(cudaMemsetAsync(spart.p, 0, sizeof(double) * 12 * (size_t)x_ctas(), stream));
         // 4. chain propagators of every species
         for (int isp = 0; isp < (int)c.sp.size(); ++isp) solve_species(isp, stress);
+        charge_fold();
         // 5. DFT of the raw densities and the ion Boltzmann factors
         fft3<-1>(dB.p, M + 1 + J);
         // 6. ion partition functions from the DC bins
