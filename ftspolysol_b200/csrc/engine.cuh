@@ -1408,7 +1408,7 @@ struct Engine : EngineBase {
     template <int N, int S1, int S2, class Op>
     void plane_ct(const V* src, V* dst, int nf, const Op& op)
     {
-        constexpr int E = F32 ? (N >= 128 ? 32 : 16) : (N >= 64 ? 16 : 8);
+        constexpr int E = F32 ? (N >= 128 ? 16 : 16) : (N >= 64 ? 16 : 8);
         constexpr int NT = N * N / E;
         auto k = k_plane_ct<T, N, RMAX, NT, E, S1, S2, Op>;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * (N + 1) + N), (size_t)4096);

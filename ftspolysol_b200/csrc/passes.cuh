@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
         __syncthreads();
     }
     op.begin();
-    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    constexpr int PB = (sizeof(T) == 4 && NT < 1024) ? 8 : 4;
 #pragma unroll 1
     for (int u0 = 0; u0 < EPT; u0 += PB) {
         typename Op::Pre pre[PB];
@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
         __syncthreads();
     }
     op.begin();
-    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    constexpr int PB = (sizeof(T) == 4 && NT < 1024) ? 8 : 4;
 #pragma unroll 1
     for (int u0 = 0; u0 < EPT; u0 += PB) {
         typename Op::Pre pre[PB];
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, 
         __syncthreads();
     }
     op.begin();
-    constexpr int PB = sizeof(T) == 4 ? 8 : 4;
+    constexpr int PB = (sizeof(T) == 4 && NT < 1024) ? 8 : 4;
 #pragma unroll 1
     for (int u0 = 0; u0 < EPT; u0 += PB) {
         typename Op::Pre pre[PB];
