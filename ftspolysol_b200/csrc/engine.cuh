@@ -1405,6 +1405,29 @@ struct Engine : EngineBase {
     // (32, 64, 128), runtime-plan kernels for every other 2/3/5-smooth grid ----
     template <int N> static constexpr bool plane_ct_ok() { return F32 ? (N == 32 || N == 64 || N == 128) : (N == 32 || N == 64); }
 
+    // Launches a pass kernel with programmatic dependent launch (the kernel
+    // waits for its predecessor with griddepcontrol.wait).
+    bool use_pdl = true;
+    template <class K, class... Args>
+    void launch_pass(K kernel, dim3 grid, int threads, size_t smem, Args... args)
+    {
+        if (!use_pdl) {
+            kernel<<<grid, threads, smem, stream>>>(args...);
+            return;
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        FTSP_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+    }
+
     template <int N, int S1, int S2, class Op>
     void plane_ct(const V* src, V* dst, int nf, const Op& op)
     {
@@ -1413,7 +1436,7 @@ struct Engine : EngineBase {
         auto k = k_plane_ct<T, N, RMAX, NT, E, S1, S2, Op>;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * (N + 1) + N), (size_t)4096);
         set_smem(k, smem);
-        k<<<dim3(c.m1, nf), NT, smem, stream>>>(src, dst, V_, tw3.p, op);
+        launch_pass(k, dim3(c.m1, nf), NT, smem, src, dst, (size_t)V_, (const V*)tw3.p, op);
         ++launches;
     }
 
@@ -1443,7 +1466,8 @@ struct Engine : EngineBase {
         const size_t smem = std::max(sizeof(V) * (size_t)(N * WCT + N), (size_t)4096);
         set_smem(k, smem);
         const int outer = DIM == 1 ? c.m1 : c.m2;
-        k<<<dim3(outer * (c.m3 / WCT), nf), NT, smem, stream>>>(c.m2, c.m3, src, dst, V_, DIM == 1 ? tw2.p : tw1.p, op);
+        launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, src, dst, (size_t)V_,
+                    (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
         ++launches;
     }
 

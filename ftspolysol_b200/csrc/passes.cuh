@@ -21,6 +21,17 @@
 
 namespace ftsp {
 
+// Programmatic dependent launch: a pass launched with the programmatic
+// stream-serialisation attribute starts while the previous kernel drains;
+// griddepcontrol.wait holds it until that kernel has completed and its
+// writes are visible, so only the prologue (constant twiddles into shared
+// memory, index set-up) overlaps.  launch_dependents lets the next pass be
+// scheduled once this CTA has issued its last global reads.  Both are no-ops
+// for launches without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+
 struct PlaneGeom {
     int m1, m2, m3;
     int P;                 // shared-memory pitch of a plane row (m3 + 1)
@@ -274,6 +285,7 @@ __global__ void __launch_bounds__(256, 2) k_strided(LineGeom g, const cplx<T>* s
             }
         }
     }
+    pdl_trigger();
     if (S2 != 0) {
         __syncthreads();
         fft_tile<V, S2, E>(tile, st, g.p, g.W, g.fW, g.W, 1);
@@ -564,6 +576,7 @@ struct OpBond {
 
 namespace ftsp {
 
+
 // ---------------------------------------------------------------------------
 // Compile-time specialisations of the three passes for production grids.
 // Same structure and Op interface as the runtime-plan kernels above; all
@@ -586,6 +599,7 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     if (S1 != 0 || S2 != 0)
         for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
     constexpr int EPT = (NE + NT - 1) / NT;   // elements per thread
     if (S1 != 0) {
         V v[EPT];   // every load of the thread in flight before the first smem store
@@ -626,6 +640,7 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
             }
         }
     }
+    pdl_trigger();
     if (S2 != 0) {
         __syncthreads();
         ct_fft<V, S2, N, RMAX, N, 1, P, NT, E>(tile, stw);
@@ -656,6 +671,7 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
     const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
     if (S1 != 0 || S2 != 0)
         for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
     constexpr int EPT = (NE + NT - 1) / NT;
     if (S1 != 0) {
         V v[EPT];
@@ -698,6 +714,7 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
             }
         }
     }
+    pdl_trigger();
     if (S2 != 0) {
         __syncthreads();
         ct_fft<V, S2, N, RMAX, W, W, 1, NT, E>(tile, stw);
