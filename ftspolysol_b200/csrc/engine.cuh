@@ -173,7 +173,9 @@ static double wave_number(int i, int m, double L)
 template <class F>
 __global__ void k_foreach(size_t n, F f)
 {
+    pdl_wait();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) f(i);
+    pdl_trigger();
 }
 
 // Sum (MAX = false) or maximum (MAX = true) of K channels; partial[block*K + c].
@@ -184,7 +186,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
     double acc[K];
 #pragma unroll
     for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    pdl_wait();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) f(i, acc);
+    pdl_trigger();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < K; ++c) {
@@ -214,6 +218,7 @@ __global__ void k_combine(const double* partial, int count, int K, double* out)
 {
     const int c = blockIdx.x;
     double s = 0.0;
+    pdl_wait();
     for (int b = threadIdx.x; b < count; b += 32) {
         const double y = partial[(size_t)b * K + c];
         s = MAX ? fmax(s, y) : s + y;
@@ -1386,7 +1391,7 @@ struct Engine : EngineBase {
     {
         const int threads = 256;
         const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 16);
-        k_foreach<<<std::max(1, blocks), threads, 0, stream>>>(n, f);
+        launch_pass(k_foreach<F>, dim3(std::max(1, blocks)), threads, 0, n, f);
         ++launches;
     }
 
@@ -1394,8 +1399,8 @@ struct Engine : EngineBase {
     template <int K, bool MAX = false, class F>
     void reduce(size_t n, F f, double* out)
     {
-        k_reduce<K, MAX><<<RED_BLOCKS, RED_THREADS, 0, stream>>>(n, f, part.p);
-        k_combine<MAX><<<K, 32, 0, stream>>>(part.p, RED_BLOCKS, K, out);
+        launch_pass(k_reduce<K, MAX, F>, dim3(RED_BLOCKS), RED_THREADS, 0, n, f, (double*)part.p);
+        launch_pass(k_combine<MAX>, dim3(K), 32, 0, (const double*)part.p, (int)RED_BLOCKS, (int)K, out);
         launches += 2;
     }
 
