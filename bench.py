@@ -61,6 +61,10 @@ def parse_args():
                     help="instead of the throughput line: this many independent replicas of uneven grids "
                          "(32^3-96^3), spread over the ranks and stepped as one CUDA graph per rank")
     ap.add_argument("--steps-per-graph", type=int, default=2)
+    ap.add_argument("--precision-report", action="store_true",
+                    help="instead of the throughput line: complex64 against complex128 on the 64^3, N = 50 "
+                         "workload, per observable (mean and standard error over 10 blocks)")
+    ap.add_argument("--report-steps", type=int, default=5000)
     return ap.parse_args()
 
 
@@ -701,6 +705,67 @@ def run_replicas(args, ws, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# precision report: complex64 propagators against complex128, same noise
+# ---------------------------------------------------------------------------
+def run_precision_report(args, local):
+    import time
+    import numpy as np
+    import torch
+    from ftspolysol_b200 import Engine, FP32, FP64, SCHEME_SI
+    from ftspolysol_b200.cases import workload
+    from ftspolysol_b200.derive import derive
+    from ftspolysol_b200.engine import NonFinite
+
+    torch.cuda.set_device(local)
+    case = workload(2, noise=True)
+    d = derive(case)
+    om, ps = case.initial_fields()
+    S, J = len(d["species"]), len(d["ions"])
+    C = S + J
+    names = ["mu_poly_ex", "H_real"] + ["stress_" + c for c in d["stress"]] + ["Pi"]
+    idx = [0, 3 * C] + [3 * C + 1 + k for k in range(len(d["stress"]))] + [3 * C + 1 + len(d["stress"])]
+    runs = {}
+    for prec, tag in ((FP64, "c128"), (FP32, "c64")):
+        e = Engine(d, precision=prec, scheme=SCHEME_SI, noise=True, seed=31, device=local)
+        e.set_fields(om, ps)
+        torch.cuda.synchronize()
+        rows, first_bad = [], None
+        t0 = time.perf_counter()
+        for k in range(args.report_steps):
+            try:
+                _, rec, _ = e.step()
+                rows.append([rec[i].real for i in idx])
+            except NonFinite:
+                first_bad = k + 1   # a runaway: the trajectory ends here
+                break
+        runs[tag] = {"rows": np.array(rows), "wall_s": time.perf_counter() - t0, "first_nonfinite_step": first_bad}
+        e.close()
+    L = min(len(runs["c128"]["rows"]), len(runs["c64"]["rows"]))
+    a, b = runs["c128"]["rows"][:L], runs["c64"]["rows"][:L]
+    start = L // 5   # equilibration discarded
+    out = {}
+    for j, n in enumerate(names):
+        def blocks(x):
+            x = x[start:, j]
+            bl = np.array_split(x, 10)
+            m = np.array([np.nanmean(q) for q in bl])
+            return float(np.nanmean(m)), float(np.nanstd(m, ddof=1) / np.sqrt(len(m)))
+        m64, s64 = blocks(a)
+        m32, s32 = blocks(b)
+        early = np.abs(b[:50, j] - a[:50, j]) / np.maximum(np.abs(a[:50, j]), 1e-12)
+        out[n] = {"c128_mean": m64, "c128_se": s64, "c64_mean": m32, "c64_se": s32,
+                  "difference": m32 - m64, "difference_in_se": (m32 - m64) / max(np.hypot(s64, s32), 1e-300),
+                  "max_rel_diff_first_50_steps": float(np.nanmax(early))}
+    print(json.dumps({"metric": "complex64 vs complex128 observables (block means)", "config": {
+        "workload": case.name + ": 64^3, L=32b, N=50, monovalent counterions, salt 0.1, semi-implicit dt 0.005, "
+                                "same noise in both runs; the steps both runs completed before a runaway, first "
+                                "20% discarded, 10 blocks"},
+        "steps_requested": args.report_steps, "steps_compared": L, "observables": out,
+        "runs": {k: {kk: vv for kk, vv in v.items() if kk != "rows"} for k, v in runs.items()}}))
+    return 0
+
+
 def derived_bytes(case, prec):
     import numpy as np
     return int(np.prod(case.m)) * (8 if prec == 1 else 16)
@@ -712,6 +777,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, ws, rank)
+        elif args.precision_report:
+            rc = run_precision_report(args, local) if rank == 0 else 0
         elif args.replicas > 0:
             rc = run_replicas(args, ws, rank, local)
         elif args.time_to_pi:
