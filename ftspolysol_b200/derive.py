@@ -19,15 +19,77 @@ import numpy as np
 from .cases import Case
 
 
+def _jacobi(K: np.ndarray):
+    """Cyclic Jacobi eigen-decomposition of a real symmetric matrix, with the
+    sweep order, rotation formulas and convergence test of the reference's
+    interactionMode::jacobi_symmetric_eigen (interactionMode.cu:122-194), so
+    that eigenvector signs, and the pivot of degenerate |components|, come
+    out as in the reference (numpy's eigh may differ in the last bit)."""
+    n = K.shape[0]
+    a = [[float(K[i, j]) for j in range(n)] for i in range(n)]
+    v = [[1.0 if i == j else 0.0 for j in range(n)] for i in range(n)]
+    if n == 1:
+        return np.array([a[0][0]]), np.array(v)
+
+    def frob(m):
+        return math.sqrt(sum(x * x for row in m for x in row))
+
+    def off(m):
+        return math.sqrt(sum(m[i][j] * m[i][j] for i in range(n) for j in range(n) if i != j))
+
+    scale = max(1.0, frob(a))
+    tol = 1e-14 * scale
+    eps = np.finfo(float).eps
+    for _ in range(max(50, 100 * n * n)):
+        if off(a) <= tol:
+            break
+        rotated = False
+        for p in range(n - 1):
+            for q in range(p + 1, n):
+                apq = a[p][q]
+                if abs(apq) <= eps * scale:
+                    continue
+                app, aqq = a[p][p], a[q][q]
+                tau = (aqq - app) / (2.0 * apq)
+                t = 1.0 / (tau + math.sqrt(1.0 + tau * tau)) if tau >= 0.0 else -1.0 / (-tau + math.sqrt(1.0 + tau * tau))
+                c = 1.0 / math.sqrt(1.0 + t * t)
+                s = t * c
+                for k in range(n):
+                    if k == p or k == q:
+                        continue
+                    akp, akq = a[k][p], a[k][q]
+                    nkp, nkq = c * akp - s * akq, s * akp + c * akq
+                    a[k][p] = a[p][k] = nkp
+                    a[k][q] = a[q][k] = nkq
+                a[p][p] = c * c * app - 2.0 * s * c * apq + s * s * aqq
+                a[q][q] = s * s * app + 2.0 * s * c * apq + c * c * aqq
+                a[p][q] = a[q][p] = 0.0
+                for k in range(n):
+                    vkp, vkq = v[k][p], v[k][q]
+                    v[k][p] = c * vkp - s * vkq
+                    v[k][q] = s * vkp + c * vkq
+                rotated = True
+        if not rotated:
+            break
+    return np.array([a[i][i] for i in range(n)]), np.array(v)
+
+
 def interaction_modes(M: int, xi: float, chi: np.ndarray, tol_rel: float):
+    """Modes of K = xi + chi (diagonal xi): eigenvalues in descending order,
+    eigenvectors as rows with the largest-|component| entry made positive
+    (first index on ties), active modes above tol_rel * max(1, max|d|)
+    (interactionMode.cu:196-263)."""
     K = xi + np.asarray(chi, dtype=np.float64).reshape(M, M)
     np.fill_diagonal(K, xi)
-    d, vec = np.linalg.eigh(K)
+    d, vec = _jacobi(K)
     order = sorted(range(M), key=lambda i: (-d[i], i))
     evals = np.array([d[i] for i in order])
     O = np.array([vec[:, i] for i in order])   # row l = eigenvector of mode l
     for l in range(M):
-        piv = int(np.argmax(np.abs(O[l])))
+        piv = 0
+        for k in range(1, M):
+            if abs(O[l, k]) > abs(O[l, piv]):
+                piv = k
         if O[l, piv] < 0.0:
             O[l] *= -1.0
     tol = tol_rel * max(1.0, float(np.max(np.abs(evals))))

@@ -12,8 +12,10 @@ cover: the polyelectrolyte chemistry of the 32^3 workload on a small ragged
 grid with injected noise; a two-type copolymer blend (two species, per-bond
 lengths, mixed charges, both mode signatures gamma = i and gamma = 1, salt
 with 2:1 stoichiometry, unmerged ion species, partial stress components);
-an uncharged two-type melt (electrostatics off); and a noise-free run of the
-unmodified reference executable for the step-loop output files.
+an uncharged two-type melt (electrostatics off); three monomer types with a
+one-bead charged species on an odd grid; dimers and monomers without
+electrostatics; and a noise-free run of the unmodified reference executable
+for the step-loop output files.
 """
 from __future__ import annotations
 
@@ -62,6 +64,27 @@ def golden_cases():
              dt=0.02, lambda_omega=[1.0], lambda_psi=0.0, Nt=3, noise=True,
              stress=("yy", "zz", "xz"), isotropic_pressure=True, init_seed=33)
     cases.append((c, 3))
+    # 4. three monomer types (three active modes of mixed signature), a
+    #    triblock with per-bond lengths, a one-bead charged species (N = 1),
+    #    counterions and salt, on an odd non-cubic grid.
+    tri = Species(name="ABC", num_chains=8, monomers=list("AABBCCC"), charges=[-1.0, 0.0, -1.0, 0.0, 1.0, 0.0, -1.0],
+                  bonds=[1.0, 0.9, 1.1, 1.0, 1.3, 0.8])
+    ion1 = Species(name="M2", num_chains=12, monomers=["C"], charges=[2.0])
+    c = Case(name="mix_m3", m=(10, 12, 9), dL=0.55, a=1.0, monomer_names=["A", "B", "C"],
+             chi=[0.0, 1.0, 0.5, 1.0, 0.0, 0.5, 0.5, 0.5, 0.0], xi=0.1, lB=1.2, species=[tri, ion1],
+             counterions={"number": "auto_neutralize", "valence": -1.0},
+             salt={"num_salt": 6, "cation_valence": 1.0, "anion_valence": -1.0},
+             dt=0.01, lambda_omega=[1.0, 0.7, 0.5], lambda_psi=1.0, Nt=3, noise=True,
+             stress=("xx", "yy", "zz", "xy", "xz", "yz"), isotropic_pressure=True, init_seed=55)
+    cases.append((c, 3))
+    # 5. short chains without electrostatics: dimers (N = 2) and monomers
+    #    (N = 1) of one type, no ions.
+    c = Case(name="short_neutral", m=(8, 8, 8), dL=0.5, a=1.0, monomer_names=["A"], chi=[0.0], xi=0.2, lB=0.0,
+             species=[Species(name="D", num_chains=40, monomers=["A", "A"], charges=[0.0, 0.0]),
+                      Species(name="S", num_chains=60, monomers=["A"], charges=[0.0])],
+             ions_enabled=False, dt=0.01, lambda_omega=[1.0], lambda_psi=0.0, Nt=3, noise=True,
+             stress=("xx", "zz", "xy"), isotropic_pressure=True, init_seed=66)
+    cases.append((c, 3))
     return cases
 
 
@@ -105,9 +128,11 @@ def load_dump(directory: str) -> dict:
     return out
 
 
-def run(outdir: str, harness: str, main_exe: str) -> None:
+def run(outdir: str, harness: str, main_exe: str, only=None) -> None:
     os.makedirs(outdir, exist_ok=True)
     for case, steps in golden_cases():
+        if only and case.name not in only:
+            continue
         work = tempfile.mkdtemp(prefix="golden_" + case.name + "_")
         paths = case.write(work)
         noise = noise_for(case, steps, seed=1000 + case.init_seed)
@@ -125,6 +150,8 @@ def run(outdir: str, harness: str, main_exe: str) -> None:
         shutil.rmtree(work)
         print("golden case", case.name, "->", len(arrays), "arrays")
 
+    if only and "pe_main" not in only:
+        return
     case = main_case()
     work = tempfile.mkdtemp(prefix="golden_main_")
     paths = case.write(work)
@@ -148,5 +175,6 @@ def run(outdir: str, harness: str, main_exe: str) -> None:
 
 if __name__ == "__main__":
     out = sys.argv[1] if len(sys.argv) > 1 else HERE
+    only = set(sys.argv[2].split(",")) if len(sys.argv) > 2 else None   # e.g. mix_m3,short_neutral
     ref = os.path.join(ROOT, "oracle", "_ref")
-    run(out, os.path.join(ref, "ref_harness"), os.path.join(ref, "main"))
+    run(out, os.path.join(ref, "ref_harness"), os.path.join(ref, "main"), only)

@@ -13,7 +13,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden  # noqa: E402
 
 
-@pytest.mark.parametrize("idx", [0, 1, 2])
+@pytest.mark.parametrize("idx", [0, 1, 2, 3, 4])
 def test_derive_matches_reference(idx, golden_dir):
     case, _ = make_golden.golden_cases()[idx]
     g = np.load(os.path.join(golden_dir, case.name + ".npz"))

@@ -13,7 +13,7 @@ import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["pe_small", "copoly_m2", "neutral_m2"]
+CASES = ["pe_small", "copoly_m2", "neutral_m2", "mix_m3", "short_neutral"]
 FIELD_TOL = 1e-10
 RECORD_TOL = 1e-10
 

@@ -77,7 +77,7 @@ def check_config(cfg, ref):
     assert cfg.isotropic_pressure == int(ref["isotropic_pressure"])
 
 
-@pytest.mark.parametrize("name", GOLDEN[:3])
+@pytest.mark.parametrize("name", GOLDEN[:3] + ["mix_m3", "short_neutral"])
 def test_loader_matches_reference_dump(name, golden_dir, tmp_path):
     g = np.load(os.path.join(golden_dir, name + ".npz"))
     m = Model(str(write_case(tmp_path, g)))

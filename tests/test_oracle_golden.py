@@ -13,7 +13,7 @@ import pytest
 
 import pyoracle as po
 
-CASES = ["pe_small", "copoly_m2", "neutral_m2"]
+CASES = ["pe_small", "copoly_m2", "neutral_m2", "mix_m3", "short_neutral"]
 FIELD_TOL = 1e-12      # relative to the field's max modulus
 RECORD_TOL = 1e-10     # relative, floor 1e-3 for values near zero
 
