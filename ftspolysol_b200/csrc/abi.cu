@@ -232,6 +232,18 @@ int ftsp_tune_info_get(ftsp_handle* h, ftsp_tune_info* info)
     return FTSP_OK;
 }
 
+int ftsp_set_adaptive(ftsp_handle* h, double u_ref)
+{
+    FTSP_GUARD(h, h->eng->set_adaptive(u_ref));
+    return FTSP_OK;
+}
+
+int ftsp_step_info(ftsp_handle* h, double* dt_eff, double* umax)
+{
+    FTSP_GUARD(h, h->eng->step_info(dt_eff, umax));
+    return FTSP_OK;
+}
+
 int ftsp_set_dt(ftsp_handle* h, double dt)
 {
     FTSP_GUARD(h, h->eng->set_dt(dt));

@@ -66,6 +66,8 @@ struct DevScal {
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
     alignas(16) unsigned long long step;   // steps taken: keys the noise, schedules the checkpoints
+    alignas(16) double dt_scale;           // this step's dt / configured dt (1 unless the step is adaptive)
+    double umax;                           // max |drift| at the start of this step (adaptive step)
     alignas(16) double lres[2];            // learned preconditioner: force residuals (learned, analytic) of the step
     alignas(16) double lres_sum[2];        // and their sums since the last statistics reset
     alignas(16) int nonfinite;
@@ -496,6 +498,8 @@ struct EngineBase {
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
     virtual long long restarts() = 0;
     virtual void set_dt(double dt) = 0;
+    virtual void set_adaptive(double u_ref) = 0;
+    virtual void step_info(double* dt_eff, double* umax) = 0;
     virtual void tune_info(ftsp_tune_info* t) = 0;
     virtual void learn_configure(const ftsp_learn_config& cf) = 0;
     virtual void learn_collect(bool on) = 0;
@@ -688,6 +692,10 @@ struct Engine : EngineBase {
         if (c.restart_interval > 0) ck.alloc((size_t)(std::max(1, c.nm) + 1) * V_);
         FTSP_CUDA(cudaMalloc(&ds, sizeof(DevScal)));
         FTSP_CUDA(cudaMemset(ds, 0, sizeof(DevScal)));
+        {
+            const double one = 1.0;
+            FTSP_CUDA(cudaMemcpy(&ds->dt_scale, &one, sizeof(double), cudaMemcpyHostToDevice));
+        }
         FTSP_CUDA(cudaMemset(omega.p, 0, sizeof(V) * nmv));
         FTSP_CUDA(cudaMemset(psi.p, 0, sizeof(V) * Vn));
         FTSP_CUDA(cudaMemset(eta.p, 0, sizeof(T) * eta.n));
@@ -990,7 +998,7 @@ struct Engine : EngineBase {
         foreach(Vn * nf, [=] __device__(size_t i) {
             const int f = (int)(i / Vn);
             const T G = (GL && d->lr_use) ? GL[i] : GA[i];
-            const V k = cscale(inc[i], (T)(1.0 / (1.0 + st.s[f] * (double)G)));
+            const V k = cscale(inc[i], (T)(1.0 / (1.0 + (st.s[f] * d->dt_scale) * (double)G)));
             if (dw) dw[i] = k;
             inc[i] = cscale(k, invV);
         });
@@ -1039,6 +1047,62 @@ struct Engine : EngineBase {
         t->candidates = tune.candidates;
         t->best_ms = tune.best_ms;
         t->default_ms = tune.default_ms;
+    }
+
+    // ---- adaptive step ----
+    // dt_eff = dt min(1, u_ref / max|u|) with max|u| the largest drift
+    // magnitude of any field at the start of the step (the adaptive step size
+    // of Aarts, James, Seiler and Stamatescu, Phys. Lett. B 687 (2010) 154, for
+    // complex Langevin runaways).  Noise amplitudes, the predictor, the
+    // corrector and the semi-implicit P(k) all use dt_eff; time averages
+    // should be weighted by it (ftsp_step_info).
+    double adaptive_u = 0.0;
+    void set_adaptive(double u_ref) override
+    {
+        if (!(u_ref >= 0.0)) throw std::runtime_error("ftsp_set_adaptive: u_ref must be >= 0");
+        adaptive_u = u_ref;
+        if (u_ref == 0.0) {
+            const double one = 1.0;
+            FTSP_CUDA(cudaMemcpyAsync(&ds->dt_scale, &one, sizeof(double), cudaMemcpyHostToDevice, stream));
+            FTSP_CUDA(cudaStreamSynchronize(stream));
+        }
+    }
+
+    void adapt_dt()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        const V* u = drift.p;
+        const V* dp = dpsi.p;
+        const bool elec = c.elec;
+        reduce<1, true>(Vn, [=] __device__(size_t i, double* acc) {
+            double m = 0.0;
+            for (int a = 0; a < nm; ++a) {
+                const double2 v = to_d(u[(size_t)a * Vn + i]);
+                m = fmax(m, v.x * v.x + v.y * v.y);
+            }
+            if (elec) {
+                const double2 v = to_d(dp[i]);
+                m = fmax(m, v.x * v.x + v.y * v.y);
+            }
+            if (!isfinite(m)) m = INFINITY;
+            acc[0] = fmax(acc[0], m);
+        }, &ds->umax);
+        DevScal* d = ds;
+        const double uref = adaptive_u;
+        k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
+            const double um = sqrt(d->umax);
+            d->umax = um;
+            d->dt_scale = (isfinite(um) && um > uref) ? uref / um : 1.0;
+        });
+        ++launches;
+    }
+
+    void step_info(double* dt_eff, double* umax) override
+    {
+        pull_scalars();
+        if (dt_eff) *dt_eff = c.dt * hs.dt_scale;
+        if (umax) *umax = hs.umax;
     }
 
     void set_dt(double dt) override
@@ -2024,7 +2088,7 @@ struct Engine : EngineBase {
             foreach(Vn, [=] __device__(size_t i) {
                 const uint64_t st = d->step;
                 for (int f = 0; f <= nm; ++f)
-                    e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)(sg.s[f] * normal_at(seed, st, (uint32_t)f, i)) : T(0);
+                    e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
             });
         }
         noise_injected = false;
@@ -2061,7 +2125,7 @@ struct Engine : EngineBase {
                     e[(size_t)nm * Vn + i] = ep;
                 }
                 for (int a = 0; a < nm; ++a) {
-                    V v = cscale(u[(size_t)a * Vn + i], (T)co.s[a]);
+                    V v = cscale(u[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale));
                     v.x += e[(size_t)a * Vn + i];
                     inc[(size_t)a * Vn + i] = v;
                 }
@@ -2069,7 +2133,7 @@ struct Engine : EngineBase {
                 if (elec) {
                     V dv = cadd(dp[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
                     dp[i] = dv;
-                    pv = cscale(dv, (T)sp);
+                    pv = cscale(dv, (T)(sp * d->dt_scale));
                     pv.x += ep;
                 }
                 inc[(size_t)nm * Vn + i] = pv;
@@ -2094,7 +2158,7 @@ struct Engine : EngineBase {
             }
             for (int a = 0; a < nm; ++a) {
                 V v = om[(size_t)a * Vn + i];
-                v = cadd(v, cscale(u[(size_t)a * Vn + i], (T)co.s[a]));
+                v = cadd(v, cscale(u[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
                 v.x += e[(size_t)a * Vn + i];
                 ob[(size_t)a * Vn + i] = v;
             }
@@ -2104,7 +2168,7 @@ struct Engine : EngineBase {
                 V dv = dp[i];
                 dv = cadd(dv, from_d<V>(md));
                 dp[i] = dv;
-                pv = cadd(ps[i], cscale(dv, (T)sp));
+                pv = cadd(ps[i], cscale(dv, (T)(sp * d->dt_scale)));
                 pv.x += ep;
             }
             pb[i] = pv;
@@ -2162,7 +2226,7 @@ struct Engine : EngineBase {
             V* inc = si_inc.p;
             foreach(Vn, [=] __device__(size_t i) {
                 for (int a = 0; a < nm; ++a) {
-                    V v = cscale(cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]), (T)co.s[a]);
+                    V v = cscale(cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]), (T)(co.s[a] * d->dt_scale));
                     v.x += e[(size_t)a * Vn + i];
                     inc[(size_t)a * Vn + i] = v;
                 }
@@ -2170,7 +2234,7 @@ struct Engine : EngineBase {
                 if (elec) {
                     const V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
                     db[i] = dbv;
-                    pv = cscale(cadd(dp[i], dbv), (T)sp);
+                    pv = cscale(cadd(dp[i], dbv), (T)(sp * d->dt_scale));
                     pv.x += e[(size_t)nm * Vn + i];
                 }
                 inc[(size_t)nm * Vn + i] = pv;
@@ -2196,8 +2260,8 @@ struct Engine : EngineBase {
             bool bad = false;
             for (int a = 0; a < nm; ++a) {
                 V w = om[(size_t)a * Vn + i];
-                w = cadd(w, cscale(u0[(size_t)a * Vn + i], (T)co.s[a]));
-                w = cadd(w, cscale(u1[(size_t)a * Vn + i], (T)co.s[a]));
+                w = cadd(w, cscale(u0[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
+                w = cadd(w, cscale(u1[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
                 w.x += e[(size_t)a * Vn + i];
                 om[(size_t)a * Vn + i] = w;
                 bad |= !(isfinite((double)w.x) && isfinite((double)w.y));
@@ -2206,8 +2270,8 @@ struct Engine : EngineBase {
             if (elec) {
                 V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
                 db[i] = dbv;
-                pv = cadd(pv, cscale(dp[i], (T)sp));
-                pv = cadd(pv, cscale(dbv, (T)sp));
+                pv = cadd(pv, cscale(dp[i], (T)(sp * d->dt_scale)));
+                pv = cadd(pv, cscale(dbv, (T)(sp * d->dt_scale)));
                 pv.x += e[(size_t)nm * Vn + i];
             } else {
                 pv = mkc<V>(T(0), T(0));
@@ -2649,8 +2713,9 @@ struct Engine : EngineBase {
             });
             ++launches;
         }
-        noises();
         drifts(0);
+        if (adaptive_u > 0.0) adapt_dt();
+        noises();
         predictor();
         eval(1, st);
         drifts(1);

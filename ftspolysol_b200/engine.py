@@ -121,6 +121,8 @@ def lib():
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
         L.ftsp_profile_read.argtypes = [vp, C.POINTER(ftsp_kernel_stat), C.c_int, C.POINTER(C.c_int)]
         L.ftsp_set_dt.argtypes = [vp, C.c_double]
+        L.ftsp_set_adaptive.argtypes = [vp, C.c_double]
+        L.ftsp_step_info.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ftsp_tune_info_get.argtypes = [vp, C.POINTER(ftsp_tune_info)]
         L.ftsp_learn_configure.argtypes = [vp, C.POINTER(ftsp_learn_config)]
         L.ftsp_learn_collect.argtypes = [vp, C.c_int]
@@ -152,7 +154,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
                "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
-               "ftsp_tune_info_get",
+               "ftsp_tune_info_get", "ftsp_set_adaptive", "ftsp_step_info",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
                "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad",
                "ftsp_batch_create", "ftsp_batch_step", "ftsp_batch_sync", "ftsp_batch_stream",
@@ -369,6 +371,16 @@ class Engine:
 
     def set_stream(self, stream_handle: int):
         self._check(lib().ftsp_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def set_adaptive(self, u_ref: float):
+        """Adaptive step: dt_eff = dt min(1, u_ref / max|u|); 0 switches it off."""
+        self._check(lib().ftsp_set_adaptive(self.h, float(u_ref)), "set_adaptive")
+
+    def step_info(self):
+        """(dt_eff, max|u|) of the last step."""
+        a, b = C.c_double(), C.c_double()
+        self._check(lib().ftsp_step_info(self.h, C.byref(a), C.byref(b)), "step_info")
+        return a.value, b.value
 
     def tune_info(self) -> dict:
         t = ftsp_tune_info()

@@ -181,6 +181,17 @@ long long ftsp_restart_count(ftsp_handle* h);
  * (param.cu:228). */
 int ftsp_set_dt(ftsp_handle* h, double dt);
 
+/* Adaptive step (no reference counterpart).  u_ref > 0: every step uses
+ * dt_eff = dt * min(1, u_ref / max|u|), max|u| being the largest drift
+ * magnitude of any field at the start of the step, in the noise amplitude,
+ * the predictor, the corrector and the semi-implicit P(k) (the adaptive step
+ * size of Aarts, James, Seiler and Stamatescu, Phys. Lett. B 687 (2010) 154,
+ * which suppresses complex-Langevin runaways).  u_ref = 0: off (the
+ * default).  ftsp_step_info returns the last step's dt_eff and max|u|
+ * (synchronises); time averages over adaptive steps are weighted by dt_eff. */
+int ftsp_set_adaptive(ftsp_handle* h, double u_ref);
+int ftsp_step_info(ftsp_handle* h, double* dt_eff, double* umax);
+
 /* Learned semi-implicit preconditioner (no reference counterpart; the
  * reference has no semi-implicit scheme).  A per-k-mode MLP (features
  * log(1+k^2), log(1+P_w(k)), log(1+P_psi(k)), N/50, lB, 10*salt; two tanh
