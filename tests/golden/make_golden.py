@@ -99,6 +99,107 @@ def main_case():
                 stress=("xx", "yy", "zz"), isotropic_pressure=True, init_seed=44)
 
 
+LEGACY_PARAM = """# legacy A/B input: no [monomers] section and no chi matrix
+[grid]
+m1 = 12
+m2 = 10
+m3 = 8
+a = 1.0
+dL = 0.5
+
+[polymer]
+species_count = 2
+sequence_file = legacy.seq
+
+[polymer.0]
+name = AB
+num_chains = 6
+N = 8
+
+[polymer.1]
+name = Bh
+num_chains = 4
+N = 5
+
+[interactions]
+xi = 0.15
+lB = 0.8
+
+[dynamics]
+dt = 0.01
+lambda_omega = 1.0
+lambdaPsi = 0.9
+Nt = 4
+Nss = 0
+Ns = 3
+Ntmp = 2
+Nso = 1
+N_stat = 1
+noise = false
+
+[ions]
+enabled = true
+[ions.counterions]
+enabled = true
+number = auto_neutralize
+valence = 1
+[ions.salt]
+enabled = true
+num_salt = 7
+cation_valence = 1
+anion_valence = -1
+combine_identical_species = false
+
+[observables]
+stress = true
+component_xy = true
+component_zz = true
+isotropic_pressure = true
+
+[output]
+step_omega_file = snap_%d.rf
+step_rhoc_file = rhoc_%d.rf
+step_ion_density_prefix = ions_%d
+"""
+
+LEGACY_SEQ = """[polymer.0]
+monomers = A A A A B B B B
+charges = -1 0 -1 0 0 -1 0 -1
+bonds = 1 1 1.2 1 1 0.9 1
+[polymer.1]
+monomers = BBBBB
+charges = -,0,-,0,-
+"""
+
+
+def legacy_inputs(seed: int = 77):
+    """Legacy two-column omega file on the full mesh and a header-less psi
+    file on half the mesh (the reference infers the mesh and resamples it)."""
+    rng = np.random.default_rng(seed)
+    m = (12, 10, 8)
+    V = 12 * 10 * 8
+    om = 0.1 * rng.standard_normal((2, V))
+    ps = 0.1 * rng.standard_normal(6 * 5 * 4)
+    return m, om, ps
+
+
+def write_legacy(work: str):
+    m, om, ps = legacy_inputs()
+    with open(os.path.join(work, "legacy.param"), "w") as f:
+        f.write(LEGACY_PARAM)
+    with open(os.path.join(work, "legacy.seq"), "w") as f:
+        f.write(LEGACY_SEQ)
+    with open(os.path.join(work, "w_ab.rf"), "w") as f:
+        f.write("%d %d %d\n" % m)
+        f.write("6 5 4\n")
+        for i in range(om.shape[1]):
+            f.write("%.12f %.12f %.12f %.12f\n" % (om[0, i], 0.0, om[1, i], 0.0))
+    with open(os.path.join(work, "psi_half.rf"), "w") as f:
+        for v in ps:
+            f.write("%.12f %.12f\n" % (v, 0.0))
+    return ["-p", "legacy.param", "--omega", "w_ab.rf", "--psi", "psi_half.rf", "-i", "run1", "-s", "out"]
+
+
 def noise_for(case: Case, steps: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     nm = case.active_mode_count()
@@ -150,6 +251,19 @@ def run(outdir: str, harness: str, main_exe: str, only=None) -> None:
         shutil.rmtree(work)
         print("golden case", case.name, "->", len(arrays), "arrays")
 
+    if not only or "legacy_main" in only:
+        work = tempfile.mkdtemp(prefix="golden_legacy_")
+        args = write_legacy(work)
+        subprocess.run([main_exe] + args, cwd=work, check=True, stdout=subprocess.DEVNULL)
+        files = {}
+        base = os.path.join(work, "out")
+        for dirpath, _, names in os.walk(base):
+            for name in names:
+                full = os.path.join(dirpath, name)
+                files["file__" + os.path.relpath(full, base)] = np.frombuffer(open(full, "rb").read(), dtype=np.uint8)
+        np.savez_compressed(os.path.join(outdir, "legacy_main.npz"), **files)
+        shutil.rmtree(work)
+        print("golden legacy run ->", sorted(files))
     if only and "pe_main" not in only:
         return
     case = main_case()

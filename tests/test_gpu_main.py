@@ -170,3 +170,28 @@ def test_restarts_from_checkpoint_then_gives_up(tmp_path):
     om = np.loadtxt(tmp_path / "tmp_omega.rf", skiprows=2)
     ref_om, _ = case.initial_fields()
     np.testing.assert_allclose(om[:, 0] + 1j * om[:, 1], np.atleast_2d(ref_om)[0], atol=1e-10)
+
+
+def test_legacy_inputs_run_directory_and_step_outputs_match_reference(tmp_path):
+    """A second run of the unmodified reference executable: legacy A/B input
+    (no [monomers], no chi: the two omega columns map to the modes), a
+    header-less psi file on half the mesh (mesh inference and trilinear
+    resampling), unmerged salt ions, a run directory (-i/-s), step outputs
+    in template folders, checkpoints every 2 steps and drift statistics
+    after step 1.  Every file the reference wrote is compared."""
+    g = np.load(os.path.join(HERE, "golden", "legacy_main.npz"))
+    args = make_golden.write_legacy(str(tmp_path))
+    run(args + ["--seed", "3"], str(tmp_path))
+    out = tmp_path / "out"
+    names = sorted(k[len("file__"):] for k in g.files)
+    mine = sorted(str(p.relative_to(out)) for p in out.rglob("*") if p.is_file())
+    assert mine == names
+    for n in names:
+        ref = bytes(g["file__" + n]).decode()
+        text = (out / n).read_text()
+        if n.endswith((".param", ".sequence")):
+            assert text == ref, n
+        elif n.endswith(".dat"):
+            compare_table(text, ref, rtol=2e-9, atol=1e-13, what=n)
+        else:
+            compare_rf(text, ref, atol=1.5e-10, what=n)
