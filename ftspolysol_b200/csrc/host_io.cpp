@@ -419,7 +419,7 @@ void usage(const char* program)
 {
     std::fprintf(stderr,
                  "usage: %s [-p param] [-i id] [-s dir] [--omega omega_file] [--psi psi_file] [--seq sequence_file] "
-                 "[--screenprint] [--fp32|--fp64] [--si|--pc] [--seed N] [--device N] [--autotune]\n",
+                 "[--screenprint] [--fp32|--fp64] [--si|--pc] [--seed N] [--device N] [--autotune] [--adaptive U]\n",
                  program);
 }
 
@@ -466,6 +466,14 @@ int parse_args(int argc, char** argv, Options& o, std::string& err)
             o.precision = FTSP_FP64;
         } else if (a == "--autotune") {
             o.autotune = 1;
+        } else if (a == "--adaptive") {
+            if (!value("--adaptive", v)) return -1;
+            char* e = nullptr;
+            o.adaptive = std::strtod(v.c_str(), &e);
+            if (e == v.c_str() || *e || !(o.adaptive >= 0.0)) {
+                err = "cannot parse --adaptive " + v;
+                return -1;
+            }
         } else if (a == "--si") {
             o.scheme = FTSP_SCHEME_SI;
         } else if (a == "--pc") {

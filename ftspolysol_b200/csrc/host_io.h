@@ -46,6 +46,7 @@ struct Options {
     bool run_id_set = false, run_parent_set = false, screenprint = false;
     // engine options (no reference counterpart)
     int precision = 0, scheme = 0, device = 0, autotune = 0;
+    double adaptive = 0.0;   // adaptive-step bound u_ref (0: fixed step)
     bool seed_set = false;
     unsigned long long seed = 0;
 };

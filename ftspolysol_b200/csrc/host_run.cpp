@@ -118,6 +118,8 @@ struct Runner {
     FILE* drift = nullptr;
     std::vector<double> obs_sum;
     long long obs_count = 0;
+    double obs_wsum = 0.0;     // sum of the step weights (adaptive step)
+    bool adaptive = false;
     bool ck_valid = false;
     int ck_step = -1;
     int restarts = 0;
@@ -176,6 +178,7 @@ struct Runner {
             if (!obs) return error("cannot open " + p.observable_file), false;
             obs_sum.assign(labels.size(), 0.0);
             obs_count = 0;
+            obs_wsum = 0.0;
             obs_header();
         }
         if (drift_enabled()) {
@@ -246,6 +249,7 @@ struct Runner {
         }
         obs_sum.clear();
         obs_count = 0;
+        obs_wsum = 0.0;
         if (!p.observable_file.empty()) {
             obs = std::fopen(p.observable_file.c_str(), "w");
             if (!obs) return error("cannot open " + p.observable_file), false;
@@ -346,10 +350,18 @@ struct Runner {
             std::fprintf(stderr, "error: non-finite value at step %d in observables\n", step);
             return 0;
         }
-        // accumulate (complexLangevin.cu:424-441)
+        // accumulate (complexLangevin.cu:424-441); with the adaptive step each
+        // record is weighted by its step dt_eff / dt (time average)
+        double wgt = 1.0;
+        if (adaptive) {
+            double dt_eff = p.dt;
+            if (!engine(ftsp_step_info(h, &dt_eff, nullptr), "step_info")) return -1;
+            wgt = p.dt > 0.0 ? dt_eff / p.dt : 1.0;
+        }
         if (step > p.Nss && obs_count < p.Ns && !obs_sum.empty()) {
+            obs_wsum += wgt;
             for (size_t c = 0; c < v.size(); ++c) {
-                obs_sum[c] += v[c];
+                obs_sum[c] += wgt * v[c];
                 if (!std::isfinite(obs_sum[c])) {
                     std::fprintf(stderr, "error: non-finite value at step %d in %s_sum\n", step, labels[c].c_str());
                     return -1;
@@ -408,7 +420,7 @@ struct Runner {
                 std::fprintf(obs, "# no_observables\n");
             } else {
                 std::vector<double> avg;
-                for (double s : obs_sum) avg.push_back(s / (double)obs_count);
+                for (double s : obs_sum) avg.push_back(adaptive ? s / obs_wsum : s / (double)obs_count);
                 write_labels(obs, "stat");
                 std::fprintf(obs, "\n");
                 std::fprintf(obs, "%*s", STEP_W, "average");
@@ -533,9 +545,12 @@ int run_main(int argc, char** argv)
     std::unique_ptr<ftsp_handle, int (*)(ftsp_handle*)> h(hraw, ftsp_destroy);
     if (ftsp_set_fields(h.get(), omega.empty() ? nullptr : omega.data(), psi.data()) != FTSP_OK)
         return error(std::string("engine: ") + ftsp_last_error(h.get())), 1;
+    if (o.adaptive > 0.0 && ftsp_set_adaptive(h.get(), o.adaptive) != FTSP_OK)
+        return error(std::string("engine: ") + ftsp_last_error(h.get())), 1;
     bool ok;
     {
         Runner run(m, h.get(), o.screenprint);
+        run.adaptive = o.adaptive > 0.0;
         ok = run.run() && run.finish();
     }
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

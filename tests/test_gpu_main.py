@@ -195,3 +195,18 @@ def test_legacy_inputs_run_directory_and_step_outputs_match_reference(tmp_path):
             compare_table(text, ref, rtol=2e-9, atol=1e-13, what=n)
         else:
             compare_rf(text, ref, atol=1.5e-10, what=n)
+
+
+def test_adaptive_step_option(tmp_path):
+    """--adaptive with a bound never reached reproduces the fixed-step run
+    file for file; a tight bound changes the trajectory and still finishes."""
+    case = small_case(Nt=5)
+    outs = []
+    for k, extra in enumerate(([], ["--adaptive", "1e30"], ["--adaptive", "0.05"])):
+        d = tmp_path / str(k)
+        paths = case.write(str(d))
+        run(["-p", os.path.basename(paths["param"]), "--omega", os.path.basename(paths["omega"]), "--psi",
+             os.path.basename(paths["psi"]), "--seed", "4"] + extra, str(d))
+        outs.append(((d / "observables.dat").read_text(), (d / "omega.rf").read_text()))
+    assert outs[0] == outs[1]
+    assert outs[2][1] != outs[0][1]
