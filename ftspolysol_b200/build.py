@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libftsp.so")
 
 SOURCES = ["engine_f32.cu", "engine_f64.cu", "abi.cu"]
 HOST_SOURCES = ["host_model.cpp", "host_io.cpp", "host_run.cpp"]
-HEADERS = ["fft_core.cuh", "passes.cuh", "learned.cuh", "engine.cuh", "host_model.h", "host_io.h"]
+HEADERS = ["fft_core.cuh", "passes.cuh", "chain_pairs.cuh", "learned.cuh", "engine.cuh", "host_model.h", "host_io.h"]
 MAIN = os.path.join(HERE, "ftsp_main")
 HOST_FLAGS = ["-O2", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-Wall"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

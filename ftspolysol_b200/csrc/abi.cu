@@ -238,6 +238,15 @@ int ftsp_set_adaptive(ftsp_handle* h, double u_ref)
     return FTSP_OK;
 }
 
+int ftsp_set_chain_symmetry(ftsp_handle* h, int on, int* n_species)
+{
+    FTSP_GUARD(h, {
+        h->eng->set_chain_symmetry(on != 0);
+        if (n_species) *n_species = h->eng->chain_symmetric_species();
+    });
+    return FTSP_OK;
+}
+
 int ftsp_step_info(ftsp_handle* h, double* dt_eff, double* umax)
 {
     FTSP_GUARD(h, h->eng->step_info(dt_eff, umax));

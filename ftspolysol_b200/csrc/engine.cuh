@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "passes.cuh"
+#include "chain_pairs.cuh"
 #include "learned.cuh"
 #include "ftsp.h"
 
@@ -499,6 +500,8 @@ struct EngineBase {
     virtual long long restarts() = 0;
     virtual void set_dt(double dt) = 0;
     virtual void set_adaptive(double u_ref) = 0;
+    virtual void set_chain_symmetry(bool on) = 0;
+    virtual int chain_symmetric_species() = 0;
     virtual void step_info(double* dt_eff, double* umax) = 0;
     virtual void tune_info(ftsp_tune_info* t) = 0;
     virtual void learn_configure(const ftsp_learn_config& cf) = 0;
@@ -565,6 +568,18 @@ struct Engine : EngineBase {
     Buf<V> ck;           // device checkpoint of (omega, psi) for rollback
     Buf<float> pmax;     // per-CTA propagator maxima, two slots (ping-pong by segment parity)
     Buf<double> spart;   // stress partials [ncta_x * 6] complex
+    // mirror-symmetric species: pair tables of the density and stress kernels
+    Buf<int2> pair_ix;
+    Buf<double> pair_wt;
+    Buf<PairRun> pair_run;
+    struct SymTables {
+        bool ok = false;
+        PairTable dens{}, stress{};
+        int dens_channels = 0;   // distinct density channels of the species
+    };
+    std::vector<SymTables> sym;
+    bool chain_sym = true;       // use the pair kernels for mirror-symmetric species
+    int qF_holds_u = -1;         // species whose u = q / E the qF buffer holds (-1: q)
     DevScal* ds = nullptr;
     DevScal hs{};
     bool noise_injected = false;
@@ -579,6 +594,7 @@ struct Engine : EngineBase {
         allocate();
         build_tables();
         plan_charge_fold();
+        plan_symmetry();
         if (c.autotune) autotune();
     }
 
@@ -590,6 +606,7 @@ struct Engine : EngineBase {
         plans.release();
         kx.release(); ky.release(); kz.release(); phi.release(); gam.release(); gion.release(); eta.release();
         part.release(); spart.release(); stage.release(); expo.release(); pmax.release();
+        pair_ix.release(); pair_wt.release(); pair_run.release();
         si_G.release(); si_inc.release(); ck.release();
         learn_release();
         if (ds) cudaFree(ds);
@@ -1103,6 +1120,14 @@ struct Engine : EngineBase {
         pull_scalars();
         if (dt_eff) *dt_eff = c.dt * hs.dt_scale;
         if (umax) *umax = hs.umax;
+    }
+
+    void set_chain_symmetry(bool on) override { chain_sym = on; }
+    int chain_symmetric_species() override
+    {
+        int n = 0;
+        for (const auto& t : sym) n += (chain_sym && t.ok) ? 1 : 0;
+        return n;
     }
 
     void set_dt(double dt) override
@@ -1695,13 +1720,16 @@ struct Engine : EngineBase {
             return r;
         };
         // ---- forward sweep ----
+        // a mirror-symmetric species stores u = q / E and needs no backward sweep
+        const bool pairs = chain_sym && sym[isp].ok;
+        qF_holds_u = pairs ? isp : -1;
         if (N == 1) {
             OpProp<T, FWD_SINGLE> op{};
             op.E = Ec(0); op.qstore = qf(0); op.partial = reinterpret_cast<double2*>(qpart); op.rn = rn(0);
             seg_pass<0, 0, FWD_SINGLE>(nullptr, nullptr, op);
         } else {
             OpProp<T, FWD_START> op0{};
-            op0.E = Ec(0); op0.qstore = qf(0); op0.rn = rn(0);
+            op0.E = Ec(0); op0.qstore = qf(0); op0.rn = rn(0); op0.store_u = pairs;
             seg_pass<0, -1, FWD_START>(nullptr, G.p, op0);
             for (int b = 0; b < N - 1; ++b) {
                 OpBond<T, true, false> ob{};
@@ -1710,12 +1738,12 @@ struct Engine : EngineBase {
                 bond_pass<-1, +1, true, false>(G.p, H.p, ob);
                 if (b + 1 < N - 1) {
                     OpProp<T, FWD_MID> op{};
-                    op.E = Ec(b + 1); op.qstore = qf(b + 1); op.rn = rn(b + 1);
+                    op.E = Ec(b + 1); op.qstore = qf(b + 1); op.rn = rn(b + 1); op.store_u = pairs;
                     seg_pass<+1, -1, FWD_MID>(H.p, G.p, op);
                 } else {
                     OpProp<T, FWD_LAST> op{};
                     op.E = Ec(b + 1); op.qstore = qf(b + 1); op.partial = reinterpret_cast<double2*>(qpart);
-                    op.rn = rn(b + 1);
+                    op.rn = rn(b + 1); op.store_u = pairs;
                     seg_pass<+1, 0, FWD_LAST>(H.p, nullptr, op);
                 }
             }
@@ -1735,6 +1763,10 @@ struct Engine : EngineBase {
                 d->Q[isp] = make_double2(ldexp(Qs.x, eF[last]), ldexp(Qs.y, eF[last]));   // true Q
             });
             launches += 2;
+        }
+        if (pairs) {
+            pair_passes(isp, stress);
+            return;
         }
         // ---- backward sweep (opposite sign convention: B' = B(-k)) ----
         auto rho_of = [&](int seg) { return dB.p + (size_t)s.type[seg] * Vn; };
@@ -1786,6 +1818,119 @@ struct Engine : EngineBase {
                 op.z = (T)s.charge[0]; op.factor = factor; op.rn = rn(0);
                 seg_pass<-1, 0, BWD_LAST>(H.p, nullptr, op);
             }
+        }
+    }
+
+    // ---- mirror-symmetric species: densities and stress from the forward sweep ----
+    void pair_passes(int isp, bool stress)
+    {
+        const Species& s = c.sp[isp];
+        const SymTables& t = sym[isp];
+        const size_t Vn = V_;
+        const int threads = 256;
+        const double2* factor = &ds->factor[isp];
+        bool charged = false;
+        for (double q : s.charge) charged |= q != 0.0;
+        V* rc = (c.elec && charged && fold_type[isp] < 0) ? dB.p + (size_t)c.M * Vn : nullptr;
+        {
+            const int blocks = (int)std::min<size_t>((Vn + threads - 1) / threads, (size_t)RED_BLOCKS);
+            cudaEvent_t ev = prof_begin();
+            launch_pass(k_pair_density<T>, dim3(blocks), threads, pair_smem(t.dens.npairs, t.dens.nruns, threads), Vn,
+                        t.dens, (const V*)qF.p, (const V*)E.p, (const int*)expo.p, s.N, factor, dB.p, rc);
+            ++launches;
+            // stored u fields, one class table per run, channel read-modify-writes
+            const int units = (s.N - 1) + t.dens.nruns + 2 * t.dens_channels + (rc ? 2 : 0);
+            prof_end(ev, "pair_density", (double)units * sizeof(V) * (double)Vn);
+        }
+        if (stress) {
+            cudaEvent_t ev = prof_begin();
+            launch_pass(k_pair_stress<T>, dim3(x_ctas()), threads, pair_smem(t.stress.npairs, t.stress.nruns, threads),
+                        c.m1, c.m2, c.m3, t.stress, (const V*)Fst.p, (const T*)phi.p, (const double*)kx.p,
+                        (const double*)ky.p, (const double*)kz.p, (const int*)expo.p, s.N, factor,
+                        reinterpret_cast<double2*>(spart.p));
+            ++launches;
+            prof_end(ev, "pair_stress", (double)(s.N - 1) * sizeof(V) * (double)Vn);
+        }
+    }
+
+    // A species is mirror-symmetric when cls[s] == cls[N-1-s] for every
+    // segment and bond b matches bond N-2-b in class and length.  Its pair
+    // tables: density pairs (s, N-1-s), s <= N-1-s, ordered by (type, class)
+    // and grouped in runs of one class; stress pairs (b, N-2-b), b <= N-2-b,
+    // grouped by bond class.  At most 1024 pairs (N <= 2048) so that the
+    // tables fit the kernels' shared memory.
+    void plan_symmetry()
+    {
+        const int S = (int)c.sp.size();
+        sym.assign(S, SymTables{});
+        std::vector<int2> ix;
+        std::vector<double> wt;
+        std::vector<PairRun> runs;
+        struct Off {
+            size_t p0, r0;
+        };
+        std::vector<Off> doff(S), soff(S);
+        for (int k = 0; k < S; ++k) {
+            const Species& sp = c.sp[k];
+            const int N = sp.N;
+            bool ok = N >= 2 && N <= 2048;
+            for (int i = 0; ok && i < N; ++i) ok = sp.cls[i] == sp.cls[N - 1 - i];
+            for (int b = 0; ok && b + 1 < N; ++b)
+                ok = sp.bcls[b] == sp.bcls[N - 2 - b] && sp.bond[b] == sp.bond[N - 2 - b];
+            if (!ok) continue;
+            SymTables& t = sym[k];
+            t.ok = true;
+            // density pairs
+            std::vector<int> seg;
+            for (int i = 0; 2 * i <= N - 1; ++i) seg.push_back(i);
+            std::stable_sort(seg.begin(), seg.end(), [&](int a, int b) {
+                return std::make_pair(sp.type[a], sp.cls[a]) < std::make_pair(sp.type[b], sp.cls[b]);
+            });
+            doff[k] = Off{ix.size(), runs.size()};
+            std::vector<int> seen(c.M, 0);
+            for (int j = 0; j < (int)seg.size(); ++j) {
+                const int i = seg[j];
+                if (j == 0 || runs.back().cls != sp.cls[i])
+                    runs.push_back(PairRun{j, j, sp.cls[i], sp.type[i], sp.charge[i]});
+                runs.back().j1 = j + 1;
+                ix.push_back(make_int2(i, N - 1 - i));
+                wt.push_back(i < N - 1 - i ? 2.0 : 1.0);
+                t.dens_channels += seen[sp.type[i]] ? 0 : 1;
+                seen[sp.type[i]] = 1;
+            }
+            t.dens.npairs = (int)seg.size();
+            t.dens.nruns = (int)(runs.size() - doff[k].r0);
+            // stress pairs
+            std::vector<int> bd;
+            for (int b = 0; 2 * b <= N - 2; ++b) bd.push_back(b);
+            std::stable_sort(bd.begin(), bd.end(), [&](int a, int b) { return sp.bcls[a] < sp.bcls[b]; });
+            soff[k] = Off{ix.size(), runs.size()};
+            for (int j = 0; j < (int)bd.size(); ++j) {
+                const int b = bd[j];
+                if (j == 0 || runs.back().cls != sp.bcls[b]) runs.push_back(PairRun{j, j, sp.bcls[b], 0, 0.0});
+                runs.back().j1 = j + 1;
+                ix.push_back(make_int2(b, N - 2 - b));
+                wt.push_back(sp.bond[b] * sp.bond[b] * (b < N - 2 - b ? 1.0 : 0.5));
+            }
+            t.stress.npairs = (int)bd.size();
+            t.stress.nruns = (int)(runs.size() - soff[k].r0);
+        }
+        if (ix.empty()) return;
+        pair_ix.alloc(ix.size());
+        pair_wt.alloc(wt.size());
+        pair_run.alloc(runs.size());
+        FTSP_CUDA(cudaMemcpy(pair_ix.p, ix.data(), sizeof(int2) * ix.size(), cudaMemcpyHostToDevice));
+        FTSP_CUDA(cudaMemcpy(pair_wt.p, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
+        FTSP_CUDA(cudaMemcpy(pair_run.p, runs.data(), sizeof(PairRun) * runs.size(), cudaMemcpyHostToDevice));
+        for (int k = 0; k < S; ++k) {
+            if (!sym[k].ok) continue;
+            SymTables& t = sym[k];
+            t.dens.pair = pair_ix.p + doff[k].p0;
+            t.dens.weight = pair_wt.p + doff[k].p0;
+            t.dens.run = pair_run.p + doff[k].r0;
+            t.stress.pair = pair_ix.p + soff[k].p0;
+            t.stress.weight = pair_wt.p + soff[k].p0;
+            t.stress.run = pair_run.p + soff[k].r0;
         }
     }
 
@@ -2575,12 +2720,27 @@ struct Engine : EngineBase {
             FTSP_CUDA(cudaMemcpyAsync(tmp.data(), p, sizeof(V) * n, cudaMemcpyDeviceToHost, stream));
             std::vector<int> ex((size_t)Nmax, 0);
             if (name == "qF") FTSP_CUDA(cudaMemcpyAsync(ex.data(), expo.p, sizeof(int) * Nmax, cudaMemcpyDeviceToHost, stream));
+            // a mirror-symmetric species stores u = q / E (u = 1 at s = 0): q = u E
+            const int su = name == "qF" ? qF_holds_u : -1;
+            std::vector<V> et;
+            if (su >= 0) {
+                et.resize(E.n);
+                FTSP_CUDA(cudaMemcpyAsync(et.data(), E.p, sizeof(V) * E.n, cudaMemcpyDeviceToHost, stream));
+            }
             FTSP_CUDA(cudaStreamSynchronize(stream));
             for (size_t i = 0; i < n; ++i) {
                 // qF is stored renormalised by 2^-aF[s]; return the true propagator
                 const int e2 = name == "qF" ? ex[i / Vn] : 0;
-                out[2 * i] = std::ldexp((double)tmp[i].x, e2);
-                out[2 * i + 1] = std::ldexp((double)tmp[i].y, e2);
+                double qx = (double)tmp[i].x, qy = (double)tmp[i].y;
+                const size_t seg = i / Vn;
+                if (su >= 0 && seg < (size_t)c.sp[su].N) {
+                    const V e = et[(size_t)c.sp[su].cls[seg] * Vn + i % Vn];
+                    const double ux = seg == 0 ? 1.0 : qx, uy = seg == 0 ? 0.0 : qy;
+                    qx = ux * (double)e.x - uy * (double)e.y;
+                    qy = ux * (double)e.y + uy * (double)e.x;
+                }
+                out[2 * i] = std::ldexp(qx, e2);
+                out[2 * i + 1] = std::ldexp(qy, e2);
             }
         }
         return (long long)(2 * n);

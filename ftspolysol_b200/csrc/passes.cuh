@@ -376,6 +376,7 @@ struct OpProp {
     const double2* factor;   // backward: species factor (n/V)/Q (Q of the stored, scaled qF)
     double2* partial;        // forward last: per-CTA sums of q
     Renorm rn;               // renormalisation (rn.eF null: off)
+    bool store_u;            // forward: store u = q / E (renormalised) instead of q
     double acc[2];
     float amax;
     T fr, fi;                // density factor (with the segment's exponent folded in)
@@ -440,7 +441,11 @@ struct OpProp {
         if (FWD) {
             V q = (KIND == FWD_START || KIND == FWD_SINGLE) ? p.e : cmul(u, p.e);
             if (KIND == FWD_MID || KIND == FWD_LAST) q = cscale(q, oscale);
-            qstore[g] = q;
+            if (store_u) {
+                if (KIND == FWD_MID || KIND == FWD_LAST) qstore[g] = cscale(u, oscale);
+            } else {
+                qstore[g] = q;
+            }
             track(q);
             if (KIND == FWD_LAST || KIND == FWD_SINGLE) {
                 acc[0] += (double)q.x;

@@ -192,6 +192,17 @@ int ftsp_set_dt(ftsp_handle* h, double dt);
 int ftsp_set_adaptive(ftsp_handle* h, double u_ref);
 int ftsp_step_info(ftsp_handle* h, double* dt_eff, double* umax);
 
+/* Mirror-symmetric chains (no reference counterpart; the reference always
+ * runs both sweeps, polymer.cu:402-416).  For a species whose segment
+ * classes and bonds read the same from both ends, q-dagger(s) = q(N-1-s),
+ * so its densities and connectivity stress are pair products over the
+ * stored forward propagators and their spectra and the backward sweep is
+ * skipped.  on = 1 (the default) uses that path for every such species;
+ * on = 0 runs both sweeps for all species.  Takes effect at the next
+ * evaluation (capture batches after setting it).  *n_species (optional)
+ * returns how many species take the pair path. */
+int ftsp_set_chain_symmetry(ftsp_handle* h, int on, int* n_species);
+
 /* Learned semi-implicit preconditioner (no reference counterpart; the
  * reference has no semi-implicit scheme).  A per-k-mode MLP (features
  * log(1+k^2), log(1+P_w(k)), log(1+P_psi(k)), N/50, lB, 10*salt; two tanh

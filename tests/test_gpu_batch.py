@@ -37,7 +37,7 @@ def test_batch_matches_individual_steps(prec, scheme, spg):
             e.step_async()
     grp = [make(c, prec, scheme, 100 + k) for k, c in enumerate(cs)]
     b = Batch(grp, spg)
-    assert b.launches_per_graph > 100 * len(cs) * spg
+    assert b.launches_per_graph > 40 * len(cs) * spg   # a whole step per replica (forward sweep alone: ~90 launches)
     for _ in range(2):   # two calls in a row
         b.step(steps // spg // 2)
     b.sync()
