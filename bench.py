@@ -326,6 +326,9 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
 
     def timed_region(profile: bool):
+        # kernels launched one by one (no step graph); with profile, every
+        # propagator pass bracketed by CUDA events
+        eng.set_step_graph(False)
         if profile:
             eng.profile(True)
         barrier(ws)
@@ -338,6 +341,7 @@ def run_ours(args, ws, rank, local):
         e1.record()
         torch.cuda.synchronize()
         barrier(ws)
+        eng.set_step_graph(True)
         return e0.elapsed_time(e1)
 
     def graph_region():

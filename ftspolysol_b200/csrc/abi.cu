@@ -146,7 +146,10 @@ const char* ftsp_last_error(const ftsp_handle* h)
 
 int ftsp_set_stream(ftsp_handle* h, void* s)
 {
-    FTSP_GUARD(h, h->eng->stream = static_cast<cudaStream_t>(s));
+    FTSP_GUARD(h, {
+        h->eng->stream = static_cast<cudaStream_t>(s);
+        h->eng->drop_step_graph();
+    });
     return FTSP_OK;
 }
 
@@ -201,7 +204,10 @@ int ftsp_set_noise(ftsp_handle* h, const double* eta)
 
 int ftsp_set_seed(ftsp_handle* h, unsigned long long seed)
 {
-    FTSP_GUARD(h, h->eng->c.seed = seed);
+    FTSP_GUARD(h, {
+        h->eng->c.seed = seed;
+        h->eng->drop_step_graph();
+    });
     return FTSP_OK;
 }
 
@@ -235,6 +241,15 @@ int ftsp_tune_info_get(ftsp_handle* h, ftsp_tune_info* info)
 int ftsp_set_adaptive(ftsp_handle* h, double u_ref)
 {
     FTSP_GUARD(h, h->eng->set_adaptive(u_ref));
+    return FTSP_OK;
+}
+
+int ftsp_set_step_graph(ftsp_handle* h, int on)
+{
+    FTSP_GUARD(h, {
+        h->eng->step_graph = on != 0;
+        h->eng->drop_step_graph();
+    });
     return FTSP_OK;
 }
 

@@ -502,6 +502,8 @@ struct EngineBase {
     virtual void set_adaptive(double u_ref) = 0;
     virtual void set_chain_symmetry(bool on) = 0;
     virtual int chain_symmetric_species() = 0;
+    virtual void drop_step_graph() = 0;
+    bool step_graph = true;   // replay a captured step in step() (see Engine::step)
     virtual void step_info(double* dt_eff, double* umax) = 0;
     virtual void tune_info(ftsp_tune_info* t) = 0;
     virtual void learn_configure(const ftsp_learn_config& cf) = 0;
@@ -600,6 +602,8 @@ struct Engine : EngineBase {
 
     ~Engine() override
     {
+        drop_step_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
         Buf<V>* vb[] = {&tw1, &tw2, &tw3, &omega, &psi, &omega_bar, &psi_bar, &drift, &drift_bar, &dpsi, &dpsi_bar,
                         &kA, &kB, &dB, &kC, &rho_p, &rho_c, &ion_rho, &E, &qF, &Fst, &G, &H};
         for (auto* b : vb) b->release();
@@ -1078,6 +1082,7 @@ struct Engine : EngineBase {
     {
         if (!(u_ref >= 0.0)) throw std::runtime_error("ftsp_set_adaptive: u_ref must be >= 0");
         adaptive_u = u_ref;
+        drop_step_graph();
         if (u_ref == 0.0) {
             const double one = 1.0;
             FTSP_CUDA(cudaMemcpyAsync(&ds->dt_scale, &one, sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -1122,7 +1127,11 @@ struct Engine : EngineBase {
         if (umax) *umax = hs.umax;
     }
 
-    void set_chain_symmetry(bool on) override { chain_sym = on; }
+    void set_chain_symmetry(bool on) override
+    {
+        chain_sym = on;
+        drop_step_graph();
+    }
     int chain_symmetric_species() override
     {
         int n = 0;
@@ -1134,10 +1143,12 @@ struct Engine : EngineBase {
     {
         if (!(dt > 0.0)) throw std::runtime_error("ftsp_set_dt: dt must be positive");
         c.dt = dt;
+        drop_step_graph();
     }
 
     void learn_configure(const ftsp_learn_config& cf) override
     {
+        drop_step_graph();
         if (c.scheme != FTSP_SCHEME_SI || !si_G.p) throw std::runtime_error("the learned preconditioner needs the semi-implicit scheme");
         const int nf = c.nm + 1;
         if (nf > mlp::NOUT_MAX) throw std::runtime_error("the learned preconditioner supports at most 3 interaction modes");
@@ -1194,6 +1205,7 @@ struct Engine : EngineBase {
 
     void learn_collect(bool on) override
     {
+        drop_step_graph();
         learn_require();
         lr.on_collect = on;
     }
@@ -1392,6 +1404,7 @@ struct Engine : EngineBase {
 
     void learn_use(bool on) override
     {
+        drop_step_graph();
         learn_require();
         if (on && !lr.trained) throw std::runtime_error("ftsp_learn_use: the network has not been trained");
         lr.on_use = on;
@@ -1420,6 +1433,7 @@ struct Engine : EngineBase {
 
     int learn_weights(float* out, int n, bool set) override
     {
+        drop_step_graph();
         learn_require();
         if (!out) return lr.np;
         if (n != lr.np) throw std::runtime_error("learned weights: expected " + std::to_string(lr.np) + " floats");
@@ -2899,10 +2913,71 @@ struct Engine : EngineBase {
         return bad ? FTSP_NONFINITE : FTSP_OK;
     }
 
+    // ---- the step as a replayed CUDA graph ----
+    // step() captures step_device() once and replays it: the step index,
+    // noise key, adaptive scale and checkpoint schedule live on the device,
+    // so every replay is the next step with fresh noise, bit-identical to
+    // launching the kernels one by one.  Steps with injected noise, with
+    // per-kernel profiling or with the learned preconditioner collecting or
+    // in use launch directly; so do steps queued while the stream is being
+    // captured by someone else (a replica batch).  Every setter that changes
+    // what a step launches drops the graph.  The capture runs on a private
+    // stream (the engine's own stream may be the legacy default stream,
+    // which cannot be captured); the graph is launched on the engine's stream.
+    cudaGraph_t sg_graph = nullptr;
+    cudaGraphExec_t sg_exec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    long long sg_launches = 0;
+
+    void drop_step_graph() override
+    {
+        if (sg_exec) cudaGraphExecDestroy(sg_exec);
+        if (sg_graph) cudaGraphDestroy(sg_graph);
+        sg_exec = nullptr;
+        sg_graph = nullptr;
+    }
+
+    bool step_graph_usable()
+    {
+        if (!step_graph || noise_injected || profiling || lr.on_collect || lr.on_use) return false;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        FTSP_CUDA(cudaStreamIsCapturing(stream, &cs));
+        return cs == cudaStreamCaptureStatusNone;
+    }
+
+    void capture_step()
+    {
+        if (!cap_stream) FTSP_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        const cudaStream_t own = stream;
+        stream = cap_stream;
+        launches = 0;
+        FTSP_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            step_device();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            stream = own;
+            throw;
+        }
+        const cudaError_t e = cudaStreamEndCapture(stream, &sg_graph);
+        stream = own;
+        FTSP_CUDA(e);
+        FTSP_CUDA(cudaGraphInstantiate(&sg_exec, sg_graph, 0));
+        sg_launches = launches;
+    }
+
     int step(double* Qbar, double* rec, double* dmax, bool sync) override
     {
         launches = 0;
-        step_device();
+        if (step_graph_usable()) {
+            if (!sg_exec) capture_step();
+            FTSP_CUDA(cudaGraphLaunch(sg_exec, stream));
+            launches = sg_launches;
+        } else {
+            step_device();
+        }
         if (!sync) return FTSP_OK;
         return read_status_impl(Qbar, rec, dmax);
     }

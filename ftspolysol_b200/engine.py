@@ -123,6 +123,7 @@ def lib():
         L.ftsp_set_dt.argtypes = [vp, C.c_double]
         L.ftsp_set_adaptive.argtypes = [vp, C.c_double]
         L.ftsp_set_chain_symmetry.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+        L.ftsp_set_step_graph.argtypes = [vp, C.c_int]
         L.ftsp_step_info.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ftsp_tune_info_get.argtypes = [vp, C.POINTER(ftsp_tune_info)]
         L.ftsp_learn_configure.argtypes = [vp, C.POINTER(ftsp_learn_config)]
@@ -155,7 +156,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
                "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
-               "ftsp_tune_info_get", "ftsp_set_adaptive", "ftsp_step_info", "ftsp_set_chain_symmetry",
+               "ftsp_tune_info_get", "ftsp_set_adaptive", "ftsp_step_info", "ftsp_set_chain_symmetry", "ftsp_set_step_graph",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
                "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad",
                "ftsp_batch_create", "ftsp_batch_step", "ftsp_batch_sync", "ftsp_batch_stream",
@@ -383,6 +384,10 @@ class Engine:
         n = C.c_int()
         self._check(lib().ftsp_set_chain_symmetry(self.h, int(bool(on)), C.byref(n)), "set_chain_symmetry")
         return n.value
+
+    def set_step_graph(self, on: bool):
+        """Replay the step as a captured CUDA graph (default on)."""
+        self._check(lib().ftsp_set_step_graph(self.h, int(bool(on))), "set_step_graph")
 
     def step_info(self):
         """(dt_eff, max|u|) of the last step."""

@@ -203,6 +203,17 @@ int ftsp_step_info(ftsp_handle* h, double* dt_eff, double* umax);
  * returns how many species take the pair path. */
 int ftsp_set_chain_symmetry(ftsp_handle* h, int on, int* n_species);
 
+/* Step as a CUDA graph (no reference counterpart).  on = 1 (the default):
+ * ftsp_step / ftsp_step_async capture the step's kernels once and replay
+ * the graph on the handle's stream (the step index, noise key, adaptive
+ * scale and checkpoint schedule are read on the device, so each replay is
+ * the next step, bit-identical to launching the kernels one by one).
+ * Steps with noise from ftsp_set_noise, with profiling on, or with the
+ * learned preconditioner collecting or in use launch directly; setters that
+ * change the step (dt, adaptive, chain symmetry, seed, stream, learned
+ * preconditioner) drop the captured graph.  on = 0: always launch directly. */
+int ftsp_set_step_graph(ftsp_handle* h, int on);
+
 /* Learned semi-implicit preconditioner (no reference counterpart; the
  * reference has no semi-implicit scheme).  A per-k-mode MLP (features
  * log(1+k^2), log(1+P_w(k)), log(1+P_psi(k)), N/50, lB, 10*salt; two tanh
