@@ -581,6 +581,7 @@ struct Engine : EngineBase {
     };
     std::vector<SymTables> sym;
     bool chain_sym = true;       // use the pair kernels for mirror-symmetric species
+    bool fused_strided = true;   // bond passes with register-resident middle stages (k_strided_fused)
     int qF_holds_u = -1;         // species whose u = q / E the qF buffer holds (-1: q)
     DevScal* ds = nullptr;
     DevScal hs{};
@@ -1570,10 +1571,20 @@ struct Engine : EngineBase {
     {
         constexpr int E = F32 ? 16 : 8;
         constexpr int NT = N * WCT / E;
-        auto k = k_strided_ct<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * WCT + N), (size_t)4096);
-        set_smem(k, smem);
         const int outer = DIM == 1 ? c.m1 : c.m2;
+        if constexpr (S1 != 0 && S2 != 0 && strided_fused_ok<N, WCT, RMAX, NT, E>()) {
+            if (fused_strided) {
+                auto k = k_strided_fused<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
+                set_smem(k, smem);
+                launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, src, dst, (size_t)V_,
+                            (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
+                ++launches;
+                return;
+            }
+        }
+        auto k = k_strided_ct<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
+        set_smem(k, smem);
         launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, src, dst, (size_t)V_,
                     (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
         ++launches;

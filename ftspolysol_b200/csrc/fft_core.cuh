@@ -401,4 +401,102 @@ __device__ __forceinline__ void ct_fft(V* tile, const V* __restrict__ tw)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Stages as separate gather / butterfly / scatter steps, for kernels that keep
+// a stage's values in registers across a pointwise step.  REV selects the
+// reversed radix order: a transform in reversed order starts with the radix
+// that the forward order ends with, and the Stockham last stage leaves each
+// thread holding positions i + t*SPAN (SPAN = N/R) of its line, which are
+// exactly the inputs i + t*M (M = N/R) of the first stage of the reversed
+// order.  So "last stage, pointwise, first stage of the next transform" runs
+// without a shared-memory round trip.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ct_rad_o(int n, int rmax, int st, bool rev)
+{
+    return ct_rad(n, rmax, rev ? ct_nst(n, rmax) - 1 - st : st);
+}
+__host__ __device__ constexpr int ct_span_o(int n, int rmax, int st, bool rev)
+{
+    int s = 1;
+    for (int k = 0; k < st; ++k) s *= ct_rad_o(n, rmax, k, rev);
+    return s;
+}
+
+// Stage ST of B lines of length N with NT threads: butterfly idx = tid + q*NT
+// (q < NB) works on line b = idx % B, butterfly i = idx / B of the line.
+template <int N, int RMAX, int B, int NT, int ST, bool REV>
+struct CtSt {
+    static constexpr int R = ct_rad_o(N, RMAX, ST, REV);
+    static constexpr int SPAN = ct_span_o(N, RMAX, ST, REV);
+    static constexpr int M = N / R;
+    static constexpr int TOTAL = B * M;
+    static constexpr int TSTEP = N / (R * SPAN);
+    static constexpr int NB = (TOTAL + NT - 1) / NT;
+    __device__ static bool valid(int q) { return TOTAL % NT == 0 || threadIdx.x + q * NT < (unsigned)TOTAL; }
+    __device__ static int butterfly(int q) { return (int)((threadIdx.x + q * NT) / B); }
+    __device__ static int line(int q) { return (int)((threadIdx.x + q * NT) % B); }
+    // position along the line of output t of butterfly q
+    __device__ static int out_pos(int q, int t)
+    {
+        const int i = butterfly(q), k = i % SPAN, kq = i / SPAN;
+        return kq * SPAN * R + k + t * SPAN;
+    }
+};
+
+template <class St, int JS, int BS, typename V>
+__device__ __forceinline__ void st_gather(const V* tile, V (&u)[St::NB][St::R])
+{
+#pragma unroll
+    for (int q = 0; q < St::NB; ++q)
+        if (St::valid(q)) {
+            const V* src = tile + St::butterfly(q) * JS + St::line(q) * BS;
+#pragma unroll
+            for (int t = 0; t < St::R; ++t) u[q][t] = src[t * St::M * JS];
+        }
+}
+
+template <int S, class St, typename V>
+__device__ __forceinline__ void st_butterfly(V (&u)[St::NB][St::R], const V* __restrict__ tw)
+{
+#pragma unroll
+    for (int q = 0; q < St::NB; ++q)
+        if (St::valid(q)) {
+            const unsigned k = (unsigned)St::butterfly(q) % St::SPAN;
+            if (St::SPAN > 1 && k) {
+                const unsigned step = k * St::TSTEP;
+#pragma unroll
+                for (int t = 1; t < St::R; ++t) u[q][t] = cmul(u[q][t], twiddle<S>(tw, t * step));
+            }
+            dftR<S, St::R>(u[q]);
+        }
+}
+
+template <class St, int JS, int BS, typename V>
+__device__ __forceinline__ void st_scatter(V* tile, const V (&u)[St::NB][St::R])
+{
+#pragma unroll
+    for (int q = 0; q < St::NB; ++q)
+        if (St::valid(q)) {
+            V* dst = tile + St::out_pos(q, 0) * JS + St::line(q) * BS;
+#pragma unroll
+            for (int t = 0; t < St::R; ++t) dst[t * St::SPAN * JS] = u[q][t];
+        }
+}
+
+// Stages [ST, END) of one transform through shared memory.
+template <typename V, int S, int N, int RMAX, int B, int JS, int BS, int NT, bool REV, int ST, int END>
+__device__ __forceinline__ void st_range(V* tile, const V* __restrict__ tw)
+{
+    if constexpr (ST < END) {
+        using St = CtSt<N, RMAX, B, NT, ST, REV>;
+        V u[St::NB][St::R];
+        st_gather<St, JS, BS>(tile, u);
+        __syncthreads();
+        st_butterfly<S, St>(u, tw);
+        st_scatter<St, JS, BS>(tile, u);
+        __syncthreads();
+        st_range<V, S, N, RMAX, B, JS, BS, NT, REV, ST + 1, END>(tile, tw);
+    }
+}
+
 }  // namespace ftsp

@@ -728,6 +728,115 @@ __global__ void __launch_bounds__(NT, 2) k_strided_ct(int m2, int m3, const cplx
     op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
 }
 
+// Strided pass with both transforms (the bond pass), shared-memory round
+// trips cut to the stages that need them.  The coalesced load of thread
+// tid (positions tid/W + u*NT/W of column tid%W) is the input set of its
+// first-stage butterflies, so stage 0 runs on the loaded registers; the
+// second transform runs in reversed radix order, so the last stage of the
+// first transform, the pointwise op and the first stage of the second stay
+// in registers; the last stage stores its outputs (positions i + t*SPAN of
+// the column) straight to global memory.  For N = 128 (radix 16 x 8) that is
+// two shared-memory round trips instead of six.  Same grid, Op interface and
+// results (up to the rounding of the second transform's radix order) as
+// k_strided_ct.
+template <int N, int W, int RMAX, int NT, int E>
+__host__ __device__ constexpr bool strided_fused_ok()
+{
+    constexpr int NST = ct_nst(N, RMAX);
+    if (NST < 2 || NT % W != 0) return false;
+    using A0 = CtSt<N, RMAX, W, NT, 0, false>;
+    using AL = CtSt<N, RMAX, W, NT, NST - 1, false>;
+    using BL = CtSt<N, RMAX, W, NT, NST - 1, true>;
+    return A0::NB * A0::R == E && (A0::M * W) % NT == 0 && A0::TOTAL % NT == 0 && BL::NB * BL::R == E &&
+           (BL::SPAN * W) % NT == 0 && BL::TOTAL % NT == 0 && AL::NB * AL::R == E && AL::TOTAL % NT == 0 &&
+           N * W == NT * E;
+}
+
+template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(NT, 2) k_strided_fused(int m2, int m3, const cplx<T>* src, cplx<T>* dst,
+                                                         size_t fstride, const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int NE = N * W;
+    constexpr int NST = ct_nst(N, RMAX);
+    static_assert(S1 != 0 && S2 != 0, "the fused pass runs both transforms");
+    static_assert(strided_fused_ok<N, W, RMAX, NT, E>(), "tile shape not supported by the fused pass");
+    using A0 = CtSt<N, RMAX, W, NT, 0, false>;          // first stage, first transform
+    using AL = CtSt<N, RMAX, W, NT, NST - 1, false>;    // last stage, first transform
+    using B0 = CtSt<N, RMAX, W, NT, 0, true>;           // first stage, second transform (radix of AL)
+    using BL = CtSt<N, RMAX, W, NT, NST - 1, true>;     // last stage, second transform
+    static_assert(B0::R == AL::R && B0::NB == AL::NB && B0::M == AL::SPAN, "stage mismatch");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + NE;
+    const int nzb = m3 / W;
+    const int outer = blockIdx.x / nzb;
+    const int z0 = (blockIdx.x - outer * nzb) * W;
+    const int f = blockIdx.y;
+    const size_t plane = (size_t)m2 * m3;
+    const size_t lstride = DIM == 1 ? (size_t)m3 : plane;
+    const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
+    for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
+    // load: value u of the thread is position tid/W + u*NT/W of column tid%W
+    V v[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int e = threadIdx.x + u * NT;
+        v[u] = src[base + (e / W) * lstride + e % W];
+    }
+    __syncthreads();   // twiddles in shared memory
+    {
+        V a[A0::NB][A0::R];
+#pragma unroll
+        for (int q = 0; q < A0::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < A0::R; ++t) a[q][t] = v[q + t * (A0::M * W / NT)];
+        st_butterfly<S1, A0>(a, stw);
+        st_scatter<A0, W, 1>(tile, a);
+        __syncthreads();
+    }
+    st_range<V, S1, N, RMAX, W, W, 1, NT, false, 1, NST - 1>(tile, stw);
+    op.begin();
+    {
+        V a[AL::NB][AL::R];
+        st_gather<AL, W, 1>(tile, a);
+        typename Op::Pre pre[AL::NB][AL::R];
+#pragma unroll
+        for (int q = 0; q < AL::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < AL::R; ++t)
+                pre[q][t] = op.load(f, base + (size_t)AL::out_pos(q, t) * lstride + AL::line(q));
+        __syncthreads();   // every gather done before the tile is rewritten
+        st_butterfly<S1, AL>(a, stw);
+#pragma unroll
+        for (int q = 0; q < AL::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < AL::R; ++t) {
+                const int j = AL::out_pos(q, t), w = AL::line(q);
+                const int x = DIM == 1 ? outer : j;
+                const int y = DIM == 1 ? j : outer;
+                a[q][t] = op.apply(f, x, y, z0 + w, base + (size_t)j * lstride + w, a[q][t], pre[q][t]);
+            }
+        pdl_trigger();
+        st_butterfly<S2, B0>(a, stw);
+        st_scatter<B0, W, 1>(tile, a);
+        __syncthreads();
+    }
+    st_range<V, S2, N, RMAX, W, W, 1, NT, true, 1, NST - 1>(tile, stw);
+    {
+        V a[BL::NB][BL::R];
+        st_gather<BL, W, 1>(tile, a);
+        st_butterfly<S2, BL>(a, stw);
+#pragma unroll
+        for (int q = 0; q < BL::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < BL::R; ++t)
+                dst[base + (size_t)BL::out_pos(q, t) * lstride + BL::line(q)] = a[q][t];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
 // z-line pass: BR rows of length N per CTA; grid (m1*m2/BR, nf).
 template <typename T, int N, int BR, int RMAX, int NT, int E, int S1, int S2, class Op>
 __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, cplx<T>* dst, size_t fstride,
