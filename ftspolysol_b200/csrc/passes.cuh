@@ -520,6 +520,10 @@ struct OpBond {
     const int* eB;
     int s, N;                // bond s -> s+1 of a species with N segments
     double acc[12];
+    // resident CTAs per SM asked of the fused bond pass: without the stress
+    // sums it fits 64 registers, so a 128^3 pass (1024 CTAs of 128 threads)
+    // runs in one wave; with them, fewer registers would spill
+    static constexpr int FUSED_MIN_BLOCKS = STRESS ? 2 : 8;
     struct Pre {
         V F;
     };
@@ -753,7 +757,7 @@ __host__ __device__ constexpr bool strided_fused_ok()
 }
 
 template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S1, int S2, class Op>
-__global__ void __launch_bounds__(NT, 2) k_strided_fused(int m2, int m3, const cplx<T>* src, cplx<T>* dst,
+__global__ void __launch_bounds__(NT, Op::FUSED_MIN_BLOCKS) k_strided_fused(int m2, int m3, const cplx<T>* src, cplx<T>* dst,
                                                          size_t fstride, const cplx<T>* __restrict__ twn, Op op)
 {
     using V = cplx<T>;
