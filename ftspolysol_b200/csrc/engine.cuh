@@ -1683,7 +1683,8 @@ struct Engine : EngineBase {
         cudaEvent_t ev = prof_begin();
         seg_pass_launch<S1, S2, KIND>(src, dst, op);
         prof_end(ev, std::string(plane_ok ? "plane_" : "zline_") + kind_name(KIND),
-                 (double)seg_units(KIND, op.rho_charge != nullptr) * sizeof(V) * (double)V_);
+                 (double)(seg_units(KIND, op.rho_charge != nullptr) - (KIND == FWD_START && op.store_u ? 1 : 0)) *
+                     sizeof(V) * (double)V_);   // u(0) = 1 is not stored
     }
 
     template <int S1, int S2, int KIND>
