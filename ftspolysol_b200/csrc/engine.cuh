@@ -582,6 +582,7 @@ struct Engine : EngineBase {
     std::vector<SymTables> sym;
     bool chain_sym = true;       // use the pair kernels for mirror-symmetric species
     bool fused_strided = true;   // bond passes with register-resident middle stages (k_strided_fused)
+    bool fused_plane = true;     // mid segment passes with register-resident end stages (k_plane_fused)
     int qF_holds_u = -1;         // species whose u = q / E the qF buffer holds (-1: q)
     DevScal* ds = nullptr;
     DevScal hs{};
@@ -1542,8 +1543,17 @@ struct Engine : EngineBase {
     {
         constexpr int E = F32 ? (N >= 128 ? 16 : 16) : (N >= 64 ? 16 : 8);
         constexpr int NT = N * N / E;
-        auto k = k_plane_ct<T, N, RMAX, NT, E, S1, S2, Op>;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * (N + 1) + N), (size_t)4096);
+        if constexpr (S1 != 0 && S2 != 0 && plane_fused_ok<N, RMAX, NT, E>()) {
+            if (fused_plane) {
+                auto k = k_plane_fused<T, N, RMAX, NT, E, S1, S2, Op>;
+                set_smem(k, smem);
+                launch_pass(k, dim3(c.m1, nf), NT, smem, src, dst, (size_t)V_, (const V*)tw3.p, op);
+                ++launches;
+                return;
+            }
+        }
+        auto k = k_plane_ct<T, N, RMAX, NT, E, S1, S2, Op>;
         set_smem(k, smem);
         launch_pass(k, dim3(c.m1, nf), NT, smem, src, dst, (size_t)V_, (const V*)tw3.p, op);
         ++launches;

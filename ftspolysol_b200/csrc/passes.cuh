@@ -659,6 +659,94 @@ __global__ void __launch_bounds__(NT, 1) k_plane_ct(const cplx<T>* src, cplx<T>*
     op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
 }
 
+// Plane pass with both transforms (the mid segment passes), two
+// shared-memory round trips fewer than k_plane_ct: the inverse transform
+// runs along y first, and the coalesced load of thread tid (rows
+// tid/N + u*NT/N of column tid%N) is the input set of its first radix stage
+// along y, so that stage runs on the loaded registers; the forward
+// transform ends along y, and its last stage stores its outputs (rows
+// i + t*SPAN of the column) straight to global memory.  Same grid, Op
+// interface and results (up to the rounding of the axis order) as
+// k_plane_ct.
+template <int N, int RMAX, int NT, int E>
+__host__ __device__ constexpr bool plane_fused_ok()
+{
+    constexpr int NST = ct_nst(N, RMAX);
+    if (NST < 2 || NT % N != 0) return false;
+    using A0 = CtSt<N, RMAX, N, NT, 0, false>;
+    using AL = CtSt<N, RMAX, N, NT, NST - 1, false>;
+    return A0::NB * A0::R == E && (A0::M * N) % NT == 0 && A0::TOTAL % NT == 0 && AL::NB * AL::R == E &&
+           AL::TOTAL % NT == 0 && N * N == NT * E;
+}
+
+template <typename T, int N, int RMAX, int NT, int E, int S1, int S2, class Op>
+__global__ void __launch_bounds__(NT, 1) k_plane_fused(const cplx<T>* src, cplx<T>* dst, size_t fstride,
+                                                       const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int P = N + 1, NE = N * N;
+    constexpr int NST = ct_nst(N, RMAX);
+    static_assert(S1 != 0 && S2 != 0, "the fused plane pass runs both transforms");
+    static_assert(plane_fused_ok<N, RMAX, NT, E>(), "plane shape not supported by the fused pass");
+    using A0 = CtSt<N, RMAX, N, NT, 0, false>;          // first y stage (line = z column)
+    using AL = CtSt<N, RMAX, N, NT, NST - 1, false>;    // last y stage
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + N * P;
+    const int x = blockIdx.x;
+    const int f = blockIdx.y;
+    const size_t base = (size_t)f * fstride + (size_t)x * NE;
+    for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
+    V v[E];   // value u: row tid/N + u*NT/N, column tid%N
+#pragma unroll
+    for (int u = 0; u < E; ++u) v[u] = src[base + threadIdx.x + u * NT];
+    __syncthreads();   // twiddles in shared memory
+    {
+        V a[A0::NB][A0::R];
+#pragma unroll
+        for (int q = 0; q < A0::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < A0::R; ++t) a[q][t] = v[q + t * (A0::M * N / NT)];
+        st_butterfly<S1, A0>(a, stw);
+        st_scatter<A0, P, 1>(tile, a);
+        __syncthreads();
+    }
+    st_range<V, S1, N, RMAX, N, P, 1, NT, false, 1, NST>(tile, stw);   // rest of y
+    ct_fft<V, S1, N, RMAX, N, 1, P, NT, E>(tile, stw);                  // z-lines
+    op.begin();
+    constexpr int EPT = NE / NT;
+    constexpr int PB = (sizeof(T) == 4 && NT < 1024) ? 8 : 4;
+#pragma unroll 1
+    for (int u0 = 0; u0 < EPT; u0 += PB) {
+        typename Op::Pre pre[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k)
+            if (u0 + k < EPT) pre[k] = op.load(f, base + threadIdx.x + (u0 + k) * NT);
+#pragma unroll
+        for (int k = 0; k < PB; ++k)
+            if (u0 + k < EPT) {
+                const int e = threadIdx.x + (u0 + k) * NT;
+                const int y = e / N, z = e % N;
+                tile[y * P + z] = op.apply(f, x, y, z, base + e, tile[y * P + z], pre[k]);
+            }
+    }
+    pdl_trigger();
+    __syncthreads();
+    ct_fft<V, S2, N, RMAX, N, 1, P, NT, E>(tile, stw);                  // z-lines
+    st_range<V, S2, N, RMAX, N, P, 1, NT, false, 0, NST - 1>(tile, stw);
+    {
+        V a[AL::NB][AL::R];
+        st_gather<AL, P, 1>(tile, a);
+        st_butterfly<S2, AL>(a, stw);
+#pragma unroll
+        for (int q = 0; q < AL::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < AL::R; ++t) dst[base + (size_t)AL::out_pos(q, t) * N + AL::line(q)] = a[q][t];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
 // Strided pass: lines of length N along y (DIM 1, outer index x) or x (DIM 0,
 // outer index y), W contiguous z-columns per tile; grid (outer * M3/W, nf).
 template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S1, int S2, class Op>
