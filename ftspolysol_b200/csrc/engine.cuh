@@ -1869,10 +1869,18 @@ struct Engine : EngineBase {
         for (double q : s.charge) charged |= q != 0.0;
         V* rc = (c.elec && charged && fold_type[isp] < 0) ? dB.p + (size_t)c.M * Vn : nullptr;
         {
-            const int blocks = (int)std::min<size_t>((Vn + threads - 1) / threads, (size_t)RED_BLOCKS);
             cudaEvent_t ev = prof_begin();
-            launch_pass(k_pair_density<T>, dim3(blocks), threads, pair_smem(t.dens.npairs, t.dens.nruns, threads), Vn,
-                        t.dens, (const V*)qF.p, (const V*)E.p, (const int*)expo.p, s.N, factor, dB.p, rc);
+            constexpr int PT = PairVec<T>::PT;
+            const size_t smem = pair_smem(t.dens.npairs, t.dens.nruns, threads);
+            if (Vn % PT == 0) {   // PT consecutive points per thread, 16-byte loads
+                const int blocks = (int)std::min<size_t>((Vn / PT + threads - 1) / threads, (size_t)RED_BLOCKS);
+                launch_pass(k_pair_density_vec<T>, dim3(blocks), threads, smem, Vn, t.dens, (const V*)qF.p,
+                            (const V*)E.p, (const int*)expo.p, s.N, factor, dB.p, rc);
+            } else {
+                const int blocks = (int)std::min<size_t>((Vn + threads - 1) / threads, (size_t)RED_BLOCKS);
+                launch_pass(k_pair_density<T>, dim3(blocks), threads, smem, Vn, t.dens, (const V*)qF.p,
+                            (const V*)E.p, (const int*)expo.p, s.N, factor, dB.p, rc);
+            }
             ++launches;
             // stored u fields, one class table per run, channel read-modify-writes
             const int units = (s.N - 1) + t.dens.nruns + 2 * t.dens_channels + (rc ? 2 : 0);
