@@ -1544,6 +1544,16 @@ struct Engine : EngineBase {
         constexpr int E = F32 ? (N >= 128 ? 16 : 16) : (N >= 64 ? 16 : 8);
         constexpr int NT = N * N / E;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * (N + 1) + N), (size_t)4096);
+        // field loads (one value per point) only: wider operators keep their batched loads
+        if constexpr (S1 == 0 && S2 != 0 && sizeof(typename Op::Pre) == sizeof(V) && plane_fused_ok<N, RMAX, NT, E>()) {
+            if (fused_plane) {
+                auto k = k_plane_load_fused<T, N, RMAX, NT, E, S2, Op>;
+                set_smem(k, smem);
+                launch_pass(k, dim3(c.m1, nf), NT, smem, dst, (size_t)V_, (const V*)tw3.p, op);
+                ++launches;
+                return;
+            }
+        }
         if constexpr (S1 != 0 && S2 != 0 && plane_fused_ok<N, RMAX, NT, E>()) {
             if (fused_plane) {
                 auto k = k_plane_fused<T, N, RMAX, NT, E, S1, S2, Op>;
@@ -1583,6 +1593,17 @@ struct Engine : EngineBase {
         constexpr int NT = N * WCT / E;
         const size_t smem = std::max(sizeof(V) * (size_t)(N * WCT + N), (size_t)4096);
         const int outer = DIM == 1 ? c.m1 : c.m2;
+        // field loads (one value per point) only: wider operators keep their batched loads
+        if constexpr (S1 == 0 && S2 != 0 && sizeof(typename Op::Pre) == sizeof(V) && strided_fused_ok<N, WCT, RMAX, NT, E>()) {
+            if (fused_strided) {
+                auto k = k_strided_load_fused<T, N, WCT, DIM, RMAX, NT, E, S2, Op>;
+                set_smem(k, smem);
+                launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, dst, (size_t)V_,
+                            (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
+                ++launches;
+                return;
+            }
+        }
         if constexpr (S1 != 0 && S2 != 0 && strided_fused_ok<N, WCT, RMAX, NT, E>()) {
             if (fused_strided) {
                 auto k = k_strided_fused<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;

@@ -929,6 +929,129 @@ __global__ void __launch_bounds__(NT, Op::FUSED_MIN_BLOCKS) k_strided_fused(int 
     op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
 }
 
+// Strided pass with one transform after the op (S1 = 0: the field loads of
+// the batched 3-D transforms).  The op's values for the loaded positions
+// (tid/W + u*NT/W of column tid%W) are the first-stage inputs, so stage 0
+// runs on registers, and the last stage stores straight to global memory.
+template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S2, class Op>
+__global__ void __launch_bounds__(NT, 2) k_strided_load_fused(int m2, int m3, cplx<T>* dst, size_t fstride,
+                                                              const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int NE = N * W;
+    constexpr int NST = ct_nst(N, RMAX);
+    static_assert(S2 != 0, "one transform");
+    static_assert(strided_fused_ok<N, W, RMAX, NT, E>(), "tile shape not supported by the fused pass");
+    using A0 = CtSt<N, RMAX, W, NT, 0, false>;
+    using AL = CtSt<N, RMAX, W, NT, NST - 1, false>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + NE;
+    const int nzb = m3 / W;
+    const int outer = blockIdx.x / nzb;
+    const int z0 = (blockIdx.x - outer * nzb) * W;
+    const int f = blockIdx.y;
+    const size_t plane = (size_t)m2 * m3;
+    const size_t lstride = DIM == 1 ? (size_t)m3 : plane;
+    const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
+    for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
+    op.begin();
+    V v[E];
+    {
+        typename Op::Pre pre[E];
+#pragma unroll
+        for (int u = 0; u < E; ++u) {
+            const int e = threadIdx.x + u * NT;
+            pre[u] = op.load(f, base + (e / W) * lstride + e % W);
+        }
+#pragma unroll
+        for (int u = 0; u < E; ++u) {
+            const int e = threadIdx.x + u * NT;
+            const int j = e / W, w = e % W;
+            const int x = DIM == 1 ? outer : j;
+            const int y = DIM == 1 ? j : outer;
+            v[u] = op.apply(f, x, y, z0 + w, base + j * lstride + w, mkc<V>(T(0), T(0)), pre[u]);
+        }
+    }
+    pdl_trigger();
+    __syncthreads();   // twiddles in shared memory
+    {
+        V a[A0::NB][A0::R];
+#pragma unroll
+        for (int q = 0; q < A0::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < A0::R; ++t) a[q][t] = v[q + t * (A0::M * W / NT)];
+        st_butterfly<S2, A0>(a, stw);
+        st_scatter<A0, W, 1>(tile, a);
+        __syncthreads();
+    }
+    st_range<V, S2, N, RMAX, W, W, 1, NT, false, 1, NST - 1>(tile, stw);
+    {
+        V a[AL::NB][AL::R];
+        st_gather<AL, W, 1>(tile, a);
+        st_butterfly<S2, AL>(a, stw);
+#pragma unroll
+        for (int q = 0; q < AL::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < AL::R; ++t)
+                dst[base + (size_t)AL::out_pos(q, t) * lstride + AL::line(q)] = a[q][t];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+// Plane pass with one transform after the op (S1 = 0): the op's values for
+// the loaded positions (rows tid/N + u*NT/N of column tid%N) are the inputs
+// of the first radix stage along y, which runs on registers; then the rest
+// of y, then z, then the plane is stored from shared memory.
+template <typename T, int N, int RMAX, int NT, int E, int S2, class Op>
+__global__ void __launch_bounds__(NT, 1) k_plane_load_fused(cplx<T>* dst, size_t fstride,
+                                                            const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int P = N + 1, NE = N * N;
+    constexpr int NST = ct_nst(N, RMAX);
+    static_assert(S2 != 0, "one transform");
+    static_assert(plane_fused_ok<N, RMAX, NT, E>(), "plane shape not supported by the fused pass");
+    using A0 = CtSt<N, RMAX, N, NT, 0, false>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + N * P;
+    const int x = blockIdx.x;
+    const int f = blockIdx.y;
+    const size_t base = (size_t)f * fstride + (size_t)x * NE;
+    for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
+    pdl_wait();
+    op.begin();
+    V v[E];
+    {
+        typename Op::Pre pre[E];
+#pragma unroll
+        for (int u = 0; u < E; ++u) pre[u] = op.load(f, base + threadIdx.x + u * NT);
+#pragma unroll
+        for (int u = 0; u < E; ++u) {
+            const int e = threadIdx.x + u * NT;
+            v[u] = op.apply(f, x, e / N, e % N, base + e, mkc<V>(T(0), T(0)), pre[u]);
+        }
+    }
+    pdl_trigger();
+    __syncthreads();   // twiddles in shared memory
+    {
+        V a[A0::NB][A0::R];
+#pragma unroll
+        for (int q = 0; q < A0::NB; ++q)
+#pragma unroll
+            for (int t = 0; t < A0::R; ++t) a[q][t] = v[q + t * (A0::M * N / NT)];
+        st_butterfly<S2, A0>(a, stw);
+        st_scatter<A0, P, 1>(tile, a);
+        __syncthreads();
+    }
+    st_range<V, S2, N, RMAX, N, P, 1, NT, false, 1, NST>(tile, stw);   // rest of y
+    ct_fft<V, S2, N, RMAX, N, 1, P, NT, E>(tile, stw);                  // z-lines
+    for (int e = threadIdx.x; e < NE; e += NT) dst[base + e] = tile[(e / N) * P + e % N];
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
 // z-line pass: BR rows of length N per CTA; grid (m1*m2/BR, nf).
 template <typename T, int N, int BR, int RMAX, int NT, int E, int S1, int S2, class Op>
 __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, cplx<T>* dst, size_t fstride,
