@@ -364,6 +364,14 @@ __device__ __forceinline__ int reduce_exponent(const float* pm, int n)
 //             propagation continues with qB[s] = u * E.
 enum PropKind { FWD_START = 0, FWD_MID = 1, FWD_LAST = 2, FWD_SINGLE = 3, BWD_START = 4, BWD_MID = 5, BWD_LAST = 6, BWD_SINGLE = 7 };
 
+// Bulk prefetch of a contiguous global range into L2 (the TMA unit's
+// non-blocking prefetch: no shared memory, no barrier, nothing to wait on).
+// Address 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void l2_prefetch_bulk(const void* p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <typename T, int KIND>
 struct OpProp {
     using V = cplx<T>;
@@ -431,6 +439,19 @@ struct OpProp {
             if (rho_charge) p.c = rho_charge[g];
         }
         return p;
+    }
+    // the operands of the pointwise step of one plane (elements g0 .. g0+n),
+    // requested at kernel start so that the loads after the inverse transform
+    // find them in L2
+    __device__ __forceinline__ void prefetch(size_t g0, unsigned n) const
+    {
+        const unsigned bytes = n * (unsigned)sizeof(V);
+        if (NEED_E) l2_prefetch_bulk(E + g0, bytes);
+        if (!FWD) {
+            l2_prefetch_bulk(qread + g0, bytes);
+            l2_prefetch_bulk(rho_type + g0, bytes);
+            if (rho_charge) l2_prefetch_bulk(rho_charge + g0, bytes);
+        }
     }
     __device__ __forceinline__ void track(V q)
     {
@@ -698,6 +719,7 @@ __global__ void __launch_bounds__(NT, 1) k_plane_fused(const cplx<T>* src, cplx<
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
     pdl_wait();
+    if (threadIdx.x == 0) op.prefetch(base, (unsigned)NE);
     V v[E];   // value u: row tid/N + u*NT/N, column tid%N
 #pragma unroll
     for (int u = 0; u < E; ++u) v[u] = src[base + threadIdx.x + u * NT];
