@@ -8,7 +8,8 @@ with FP64 reductions).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one full predictor-corrector CL step (two density evaluations,
-both chain-propagator sweeps, observables, update).  Under torchrun each rank
+each one forward chain sweep plus the pair-density and pair-stress kernels,
+since the uniform chain is mirror-symmetric; observables; update).  Under torchrun each rank
 runs its own independent replica (different seed): weak scaling, no
 collective in the data path; the elapsed time is the max over ranks.
 
@@ -246,13 +247,8 @@ def run_reference(args, ws, rank):
         return 0
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     base = {"metric": METRIC, "unit": UNIT, "impl": "reference"}
-    if not os.path.exists(harness):
-        ref_src = "/root/reference"
-        if os.path.isdir(ref_src):
-            subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh"), ref_src], check=False,
-                           stdout=subprocess.DEVNULL)
-    if not os.path.exists(harness):
-        base["unavailable"] = "reference CUDA build (oracle/_ref/ref_harness) is missing and cannot be built here"
+    if not os.path.exists(harness):   # built by __graft_entry__.build() next to the reference sources
+        base["unavailable"] = "reference CUDA build (oracle/_ref/ref_harness) is missing (run the build step first)"
         print(json.dumps(base))
         return 0
     from ftspolysol_b200.cases import workload
