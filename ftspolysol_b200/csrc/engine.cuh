@@ -584,6 +584,11 @@ struct Engine : EngineBase {
     bool fused_strided = true;   // bond passes with register-resident middle stages (k_strided_fused)
     bool fused_plane = true;     // mid segment passes with register-resident end stages (k_plane_fused)
     int qF_holds_u = -1;         // species whose u = q / E the qF buffer holds (-1: q)
+    // a single mirror-symmetric species runs its stress kernel on a second
+    // stream, overlapped with the rest of the density evaluation
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool aux_pending = false;
     DevScal* ds = nullptr;
     DevScal hs{};
     bool noise_injected = false;
@@ -606,6 +611,9 @@ struct Engine : EngineBase {
     {
         drop_step_graph();
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (aux) cudaStreamDestroy(aux);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         Buf<V>* vb[] = {&tw1, &tw2, &tw3, &omega, &psi, &omega_bar, &psi_bar, &drift, &drift_bar, &dpsi, &dpsi_bar,
                         &kA, &kB, &dB, &kC, &rho_p, &rho_c, &ion_rho, &E, &qF, &Fst, &G, &H};
         for (auto* b : vb) b->release();
@@ -1889,6 +1897,34 @@ struct Engine : EngineBase {
         bool charged = false;
         for (double q : s.charge) charged |= q != 0.0;
         V* rc = (c.elec && charged && fold_type[isp] < 0) ? dB.p + (size_t)c.M * Vn : nullptr;
+        if (stress) {
+            const size_t sm = pair_smem(t.stress.npairs, t.stress.nruns, threads);
+            // with one species nothing else reads the spectra or writes the
+            // stress partials before the record is finalised: run the kernel
+            // beside the rest of the evaluation (joined at its end)
+            if (c.sp.size() == 1 && !profiling) {
+                if (!aux) {
+                    FTSP_CUDA(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+                    FTSP_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+                    FTSP_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+                }
+                FTSP_CUDA(cudaEventRecord(ev_fork, stream));
+                FTSP_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+                k_pair_stress<T><<<x_ctas(), threads, sm, aux>>>(
+                    c.m1, c.m2, c.m3, t.stress, (const V*)Fst.p, (const T*)phi.p, (const double*)kx.p,
+                    (const double*)ky.p, (const double*)kz.p, (const int*)expo.p, s.N, factor,
+                    reinterpret_cast<double2*>(spart.p));
+                FTSP_CUDA(cudaGetLastError());
+                aux_pending = true;
+            } else {
+                cudaEvent_t ev = prof_begin();
+                launch_pass(k_pair_stress<T>, dim3(x_ctas()), threads, sm, c.m1, c.m2, c.m3, t.stress,
+                            (const V*)Fst.p, (const T*)phi.p, (const double*)kx.p, (const double*)ky.p,
+                            (const double*)kz.p, (const int*)expo.p, s.N, factor, reinterpret_cast<double2*>(spart.p));
+                prof_end(ev, "pair_stress", (double)(s.N - 1) * sizeof(V) * (double)Vn);
+            }
+            ++launches;
+        }
         {
             cudaEvent_t ev = prof_begin();
             constexpr int PT = PairVec<T>::PT;
@@ -1906,15 +1942,6 @@ struct Engine : EngineBase {
             // stored u fields, one class table per run, channel read-modify-writes
             const int units = (s.N - 1) + t.dens.nruns + 2 * t.dens_channels + (rc ? 2 : 0);
             prof_end(ev, "pair_density", (double)units * sizeof(V) * (double)Vn);
-        }
-        if (stress) {
-            cudaEvent_t ev = prof_begin();
-            launch_pass(k_pair_stress<T>, dim3(x_ctas()), threads, pair_smem(t.stress.npairs, t.stress.nruns, threads),
-                        c.m1, c.m2, c.m3, t.stress, (const V*)Fst.p, (const T*)phi.p, (const double*)kx.p,
-                        (const double*)ky.p, (const double*)kz.p, (const int*)expo.p, s.N, factor,
-                        reinterpret_cast<double2*>(spart.p));
-            ++launches;
-            prof_end(ev, "pair_stress", (double)(s.N - 1) * sizeof(V) * (double)Vn);
         }
     }
 
@@ -2250,6 +2277,11 @@ struct Engine : EngineBase {
         // when electrostatics are off the charge fields stay zero
         if (!elec) {
             FTSP_CUDA(cudaMemsetAsync(kC.p + (size_t)M * Vn, 0, sizeof(V) * 2 * Vn, stream));
+        }
+        if (aux_pending) {   // the stress kernel of the pair path
+            FTSP_CUDA(cudaEventRecord(ev_join, aux));
+            FTSP_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
+            aux_pending = false;
         }
     }
 
