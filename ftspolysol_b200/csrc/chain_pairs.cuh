@@ -162,6 +162,16 @@ struct PairVec<float> {
         o[2] = mkc<cplx<float>>(b.x, b.y);
         o[3] = mkc<cplx<float>>(b.z, b.w);
     }
+    // read-modify-write operands (the density channels): plain loads
+    __device__ static void load_rw(const cplx<float>* p, cplx<float> (&o)[4])
+    {
+        const float4 a = reinterpret_cast<const float4*>(p)[0];
+        const float4 b = reinterpret_cast<const float4*>(p)[1];
+        o[0] = mkc<cplx<float>>(a.x, a.y);
+        o[1] = mkc<cplx<float>>(a.z, a.w);
+        o[2] = mkc<cplx<float>>(b.x, b.y);
+        o[3] = mkc<cplx<float>>(b.z, b.w);
+    }
     __device__ static void store(cplx<float>* p, const cplx<float> (&o)[4])
     {
         reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
@@ -176,6 +186,7 @@ struct PairVec<double> {
         o[0] = p[0];
         o[1] = p[1];
     }
+    __device__ static void load_rw(const cplx<double>* p, cplx<double> (&o)[2]) { load(p, o); }
     __device__ static void store(cplx<double>* p, const cplx<double> (&o)[2])
     {
         p[0] = o[0];
@@ -244,7 +255,7 @@ __global__ void __launch_bounds__(256) k_pair_density_vec(size_t n, PairTable tb
             if (r + 1 == tb.nruns || sr[r + 1].type != R.type) {
                 V* d = rho + (size_t)R.type * n + i;
                 V o[PT];
-                PV::load(d, o);
+                PV::load_rw(d, o);
 #pragma unroll
                 for (int k = 0; k < PT; ++k) {
                     o[k] = mkc<V>(o[k].x + (T)(ax[k] * fc.x - ay[k] * fc.y), o[k].y + (T)(ax[k] * fc.y + ay[k] * fc.x));
@@ -255,7 +266,7 @@ __global__ void __launch_bounds__(256) k_pair_density_vec(size_t n, PairTable tb
         }
         if (rho_charge) {
             V o[PT];
-            PV::load(rho_charge + i, o);
+            PV::load_rw(rho_charge + i, o);
 #pragma unroll
             for (int k = 0; k < PT; ++k)
                 o[k] = mkc<V>(o[k].x + (T)(cx[k] * fc.x - cy[k] * fc.y), o[k].y + (T)(cx[k] * fc.y + cy[k] * fc.x));
