@@ -131,6 +131,21 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def step_roofline(prop_bytes, field, steps, npts, s_c, steps_per_s_gpu, peak):
+    """Whole-step roofline: algorithmic bytes of one step = the propagator and
+    pair passes (per-pass accounting in the engine) + the field-level passes
+    (batched transforms, elementwise and reduction kernels, each counted by
+    the fields it reads and writes), K_f = the latter in full-field units."""
+    fbytes = sum(v["bytes"] for v in field.values()) / steps
+    pbytes = prop_bytes / steps
+    total = pbytes + fbytes
+    achieved = total * steps_per_s_gpu / 1e9
+    return {"bytes_per_step": total, "propagator_bytes_per_step": pbytes, "field_bytes_per_step": fbytes,
+            "K_f": fbytes / (npts * s_c), "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
+            "field_kinds": {k: {"launches": v["launches"] / steps, "bytes": v["bytes"] / steps}
+                            for k, v in sorted(field.items())}}
+
+
 def committed_traffic():
     """Per-launch DRAM bytes of the propagator passes from the committed ncu
     summary (profiles/propagator_passes_128cube_N50.md, lines 'traffic <kind> <bytes>')."""
@@ -384,6 +399,8 @@ def run_ours(args, ws, rank, local):
 
     # roofline of the dominant propagator pass (largest total device time)
     peak, peak_kind = measured_peak_hbm()
+    field = {k: v for k, v in prof.items() if k.startswith("field_")}
+    prof = {k: v for k, v in prof.items() if not k.startswith("field_")}
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
     dname, dstat = dom
     per_launch_ms = dstat["ms"] / dstat["launches"]
@@ -398,6 +415,8 @@ def run_ours(args, ws, rank, local):
                 "traffic": traffic, "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
                 "timing": "per-kernel CUDA events over a second timed region of %d steps (%.2f ms/step with "
                           "the events, %.2f ms/step without)" % (args.steps, ms_prof / args.steps, ms / args.steps),
+                "step": step_roofline(prop_bytes, field, args.steps, eng.size, 8 if prec == FP32 else 16,
+                                      value / ws, peak),
                 "all_propagator_passes": {"achieved": prop_bytes / (prop_ms * 1e-3) / 1e9,
                                           "share_of_step": prop_ms / ms_prof,
                                           "per_kind": {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / v["launches"],

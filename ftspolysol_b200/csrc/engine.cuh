@@ -1032,7 +1032,7 @@ struct Engine : EngineBase {
             const V k = cscale(inc[i], (T)(1.0 / (1.0 + (st.s[f] * d->dt_scale) * (double)G)));
             if (dw) dw[i] = k;
             inc[i] = cscale(k, invV);
-        });
+        }, (double)(2 * sizeof(V) + sizeof(T)));
         fft3<+1>(si_inc.p, nf);
     }
 
@@ -1119,7 +1119,7 @@ struct Engine : EngineBase {
             }
             if (!isfinite(m)) m = INFINITY;
             acc[0] = fmax(acc[0], m);
-        }, &ds->umax);
+        }, &ds->umax, (double)(c.nm + 1) * sizeof(V));
         DevScal* d = ds;
         const double uref = adaptive_u;
         k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
@@ -1499,22 +1499,29 @@ struct Engine : EngineBase {
     }
 
     // ---- launch helpers ----
+    // bpe: algorithmic bytes per element (fields read + written), recorded
+    // as "field_elementwise" / "field_reduce" when profiling, so that the
+    // bytes of a whole step are known (0: not counted, set-up work only)
     template <class F>
-    void foreach(size_t n, F f)
+    void foreach(size_t n, F f, double bpe = 0.0)
     {
         const int threads = 256;
         const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 16);
+        cudaEvent_t ev = bpe > 0.0 ? prof_begin() : nullptr;
         launch_pass(k_foreach<F>, dim3(std::max(1, blocks)), threads, 0, n, f);
         ++launches;
+        prof_end(ev, "field_elementwise", bpe * (double)n);
     }
 
     // Reduce K channels over n items into out[0..K) (device memory).
     template <int K, bool MAX = false, class F>
-    void reduce(size_t n, F f, double* out)
+    void reduce(size_t n, F f, double* out, double bpe = 0.0)
     {
+        cudaEvent_t ev = bpe > 0.0 ? prof_begin() : nullptr;
         launch_pass(k_reduce<K, MAX, F>, dim3(RED_BLOCKS), RED_THREADS, 0, n, f, (double*)part.p);
         launch_pass(k_combine<MAX>, dim3(K), 32, 0, (const double*)part.p, (int)RED_BLOCKS, (int)K, out);
         launches += 2;
+        prof_end(ev, "field_reduce", bpe * (double)n);
     }
 
     // Batched in-place (or out-of-place from per-field sources) 3-D FFT of nf
@@ -1685,6 +1692,7 @@ struct Engine : EngineBase {
         OpLoad self{};
         for (int f = 0; f < nf; ++f) self.s[f] = dst + (size_t)f * V_;
         self.fs = V_;
+        cudaEvent_t ev = prof_begin();
         if (plane_ok) {
             plane<0, S>(nullptr, dst, nf, in);
         } else {
@@ -1692,6 +1700,8 @@ struct Engine : EngineBase {
             strided<1, 0, S>(nullptr, dst, nf, self);
         }
         strided<0, 0, S>(nullptr, dst, nf, self);
+        // two passes (three without the plane pass), each reading and writing every field
+        prof_end(ev, "field_fft", (plane_ok ? 4.0 : 6.0) * nf * sizeof(V) * (double)V_);
     }
 
     // Real-space pass of one segment: [inverse S1] op [forward S2] with the
@@ -2090,7 +2100,7 @@ struct Engine : EngineBase {
             V acc = dBp[(size_t)M * Vn + i];
             for (int k = 0; k < n; ++k) acc = cadd(acc, cscale(dBp[(size_t)ft.type[k] * Vn + i], (T)ft.z[k]));
             dBp[(size_t)M * Vn + i] = acc;
-        });
+        }, (2.0 + n) * sizeof(V));
     }
 
     // ---- densities at (omega_w, psi_w) ----
@@ -2139,7 +2149,7 @@ struct Engine : EngineBase {
                     const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
                     kBp[(size_t)(M + 1 + j) * Vn + i] = from_d<V>(elec ? dscale(P, gj) : make_double2(0.0, 0.0));
                 }
-            });
+            }, (double)(c.nm + 1 + c.M + 1 + J) * sizeof(V));
         }
         fft3<+1>(kB.p, M + 1 + J);
         // 3. class tables exp(-(W_type + i z psi_s)), ion Boltzmann factors, zeroed accumulators
@@ -2173,7 +2183,7 @@ struct Engine : EngineBase {
                     const T zz = (T)zi.z[j];
                     dBp[(size_t)(M + 1 + j) * Vn + i] = cexpT(zz * pj.y, -zz * pj.x);
                 }
-            });
+            }, (double)(2 * (c.M + 1 + J) + (int)c.cls.size()) * sizeof(V));
         }
         if (stress) FTSP_CUDA(cudaMemsetAsync(spart.p, 0, sizeof(double) * 12 * (size_t)x_ctas(), stream));
         // 4. chain propagators of every species
@@ -2227,7 +2237,7 @@ struct Engine : EngineBase {
                 kCp[(size_t)(M + 1) * Vn + i] = from_d<V>(ci);
                 const double k2 = kxp[x] * kxp[x] + kyp[y] * kyp[y] + kzp[z] * kzp[z];
                 kCp[(size_t)(M + 2) * Vn + i] = from_d<V>(dscale(to_d(kAp[(size_t)nm * Vn + i]), k2 * invV * dpsi_scale));
-            });
+            }, (double)(2 * c.M + 5 + J) * sizeof(V));
         }
         fft3<+1>(kC.p, M + 3);
         // 8. real-space epilogue: rho_p, rho_c, ion densities, raw psi drift (+ its sum)
@@ -2272,7 +2282,7 @@ struct Engine : EngineBase {
                 dp[i] = dv;
                 acc[0] += (double)dv.x;
                 acc[1] += (double)dv.y;
-            }, reinterpret_cast<double*>(&ds->mean_dpsi));
+            }, reinterpret_cast<double*>(&ds->mean_dpsi), (double)(c.M + 6 + 2 * J) * sizeof(V));
         }
         // when electrostatics are off the charge fields stay zero
         if (!elec) {
@@ -2310,7 +2320,7 @@ struct Engine : EngineBase {
                 acc[2 * a] += wd.x * wd.x - wd.y * wd.y;
                 acc[2 * a + 1] += 2.0 * wd.x * wd.y;
             }
-        }, ds->fsq);
+        }, ds->fsq, (double)(2 * c.nm + c.M) * sizeof(V));
     }
 
     // ---- noise for this step (generated, or injected by ftsp_set_noise) ----
@@ -2331,12 +2341,12 @@ struct Engine : EngineBase {
                 const uint64_t st = d->step;
                 for (int f = 0; f <= nm; ++f)
                     e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
-            });
+            }, (double)(c.nm + 1) * sizeof(T));
         }
         noise_injected = false;
         if (c.elec) {   // remove_real_mean of the psi noise (complexLangevin.cu:296)
             const T* ep = e + (size_t)nm * Vn;
-            reduce<1>(Vn, [=] __device__(size_t i, double* acc) { acc[0] += (double)ep[i]; }, &ds->mean_eta);
+            reduce<1>(Vn, [=] __device__(size_t i, double* acc) { acc[0] += (double)ep[i]; }, &ds->mean_eta, (double)sizeof(T));
         }
     }
 
@@ -2379,7 +2389,7 @@ struct Engine : EngineBase {
                     pv.x += ep;
                 }
                 inc[(size_t)nm * Vn + i] = pv;
-            });
+            }, (double)(c.nm * (2 * sizeof(V) + sizeof(T)) + 2 * sizeof(T) + 3 * sizeof(V)));
             si_precondition(lr.on_collect || lr.on_use);
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
                 for (int a = 0; a < nm; ++a) ob[(size_t)a * Vn + i] = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
@@ -2387,7 +2397,7 @@ struct Engine : EngineBase {
                 pb[i] = pv;
                 acc[0] += (double)pv.x;
                 acc[1] += (double)pv.y;
-            }, reinterpret_cast<double*>(&ds->mean_psi));
+            }, reinterpret_cast<double*>(&ds->mean_psi), (double)(3 * c.nm + 3) * sizeof(V));
             remove_mean(psi_bar.p, &ds->mean_psi);
             return;
         }
@@ -2416,7 +2426,7 @@ struct Engine : EngineBase {
             pb[i] = pv;
             acc[0] += (double)pv.x;
             acc[1] += (double)pv.y;
-        }, reinterpret_cast<double*>(&ds->mean_psi));
+        }, reinterpret_cast<double*>(&ds->mean_psi), (double)(c.nm * (3 * sizeof(V) + sizeof(T)) + 2 * sizeof(T) + 4 * sizeof(V)));
         remove_mean(psi_bar.p, &ds->mean_psi);
     }
 
@@ -2428,7 +2438,7 @@ struct Engine : EngineBase {
         foreach(V_, [=] __device__(size_t i) {
             const double2 m = dscale(*sum, -invV);
             f[i] = cadd(f[i], from_d<V>(m));
-        });
+        }, 2.0 * sizeof(V));
     }
 
     // ---- corrector (complexLangevin.cu:349-368) + drift maxima + finite flag ----
@@ -2463,7 +2473,7 @@ struct Engine : EngineBase {
             double v = (double)s.x * s.x + (double)s.y * s.y;
             if (!isfinite(v)) v = INFINITY;
             acc[nm] = fmax(acc[nm], v);
-        }, ds->dmax);
+        }, ds->dmax, (double)(2 * c.nm + 2) * sizeof(V));
         if (c.scheme == FTSP_SCHEME_SI) {
             V* inc = si_inc.p;
             foreach(Vn, [=] __device__(size_t i) {
@@ -2480,7 +2490,7 @@ struct Engine : EngineBase {
                     pv.x += e[(size_t)nm * Vn + i];
                 }
                 inc[(size_t)nm * Vn + i] = pv;
-            });
+            }, (double)(c.nm * (3 * sizeof(V) + sizeof(T)) + 4 * sizeof(V) + sizeof(T)));
             si_precondition();
             reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
                 bool bad = false;
@@ -2494,7 +2504,7 @@ struct Engine : EngineBase {
                 acc[0] += (double)pv.x;
                 acc[1] += (double)pv.y;
                 if (bad || !(isfinite((double)pv.x) && isfinite((double)pv.y))) acc[2] += 1.0;
-            }, ds->corr);
+            }, ds->corr, (double)(3 * c.nm + 3) * sizeof(V));
             remove_mean(psi.p, reinterpret_cast<const double2*>(ds->corr));
             return;
         }
@@ -2522,7 +2532,7 @@ struct Engine : EngineBase {
             acc[0] += (double)pv.x;
             acc[1] += (double)pv.y;
             if (bad || !(isfinite((double)pv.x) && isfinite((double)pv.y))) acc[2] += 1.0;
-        }, ds->corr);
+        }, ds->corr, (double)(c.nm * (4 * sizeof(V) + sizeof(T)) + 5 * sizeof(V) + sizeof(T)));
         remove_mean(psi.p, reinterpret_cast<const double2*>(ds->corr));
     }
 
@@ -2592,7 +2602,7 @@ struct Engine : EngineBase {
             }
             acc[12] += 0.5 * A.x + Bc.x / 6.0 + I0.x;
             acc[13] += 0.5 * A.y + Bc.y / 6.0 + I0.y;
-        }, ds->kobs);
+        }, ds->kobs, (double)(c.nm + c.M + 2 + (int)c.ions.size()) * sizeof(V));
     }
 
     void finalize_record(bool with_stress)
@@ -2951,7 +2961,7 @@ struct Engine : EngineBase {
             if (d->bad_last || d->step % every != 0) return;
             for (int a = 0; a < nm; ++a) ckp[(size_t)a * Vn + i] = om[(size_t)a * Vn + i];
             ckp[(size_t)nm * Vn + i] = ps[i];
-        });
+        }, 2.0 * (c.nm + 1) * sizeof(V) / (double)c.restart_interval);
     }
 
     void step_device()
