@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-line", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT segment-step comparison")
     ap.add_argument("--no-graph", action="store_true",
                     help="time the steps as individual launches instead of replaying a captured CUDA graph")
     ap.add_argument("--time-to-pi", action="store_true",
@@ -212,46 +213,33 @@ def barrier(ws: int):
 # ---------------------------------------------------------------------------
 # CPU baseline: the FP64 oracle on the host cores
 # ---------------------------------------------------------------------------
-def cpu_baseline(case, derived):
+def cpu_baseline(case, derived, steps=2):
+    """The FP64 oracle (the reference's step restated in C, OpenMP over all
+    host cores) timed on `steps` full predictor-corrector steps of the
+    workload itself, with noise and the full stress tensor and pressure (its
+    observables re-solve the chains per component, as the reference does)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
     import pyoracle as po
     po.build()
     threads = po.lib().oracle_threads()
-    # cost ratio full step / one density evaluation, measured on a small grid
-    # of the same chemistry
-    from ftspolysol_b200.cases import workload
-    from ftspolysol_b200.derive import derive
-    small = workload(4, noise=False)
-    small.m = (32, 32, 32)
-    small.salt = dict(small.salt)
-    V = (32 * small.dL) ** 3
-    small.species[0].num_chains = int(round(0.5 * V / 50))
-    small.salt["num_salt"] = int(round(0.05 * V))
-    ds = derive(small)
-    o = po.Oracle(ds)
-    om, ps = small.initial_fields()
-    o.set_fields(om, ps)
-    t0 = time.perf_counter()
-    o.compute_densities(0)
-    t1 = time.perf_counter()
-    o.step(None)
-    t2 = time.perf_counter()
-    ratio = (t2 - t1) / (t1 - t0)
-    o.close()
-    # the workload itself: one density evaluation at full size
     o = po.Oracle(derived)
     om, ps = case.initial_fields()
     o.set_fields(om, ps)
-    t0 = time.perf_counter()
-    o.compute_densities(0)
-    t_dens = time.perf_counter() - t0
+    sigma = np.sqrt(2.0 * derived["dt"] / derived["dV"])
+    rng = np.random.default_rng(3)
+    times = []
+    for _ in range(steps):
+        eta = rng.standard_normal((len(derived["modes"]) + 1, case.size)) * sigma
+        t0 = time.perf_counter()
+        o.step(eta)
+        times.append(time.perf_counter() - t0)
     o.close()
-    step_s = t_dens * ratio
+    step_s = sum(times) / len(times)
     return {"value": 1.0 / step_s, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": ("one FP64 density evaluation of the 128^3 N=50 workload (%.1f s) times the measured "
-                       "full-step/density-evaluation cost ratio of the oracle (%.2f, on 32^3 N=50 of the same "
-                       "chemistry); the oracle restates the reference's step including its stress re-solves"
-                       % (t_dens, ratio))}
+            "sample": ("%d full FP64 predictor-corrector steps of the %s workload (%.1f s each, %s), timed one by "
+                       "one; the oracle restates the reference's step including its per-component stress re-solves"
+                       % (steps, case.name, step_s, ", ".join("%.1f" % t for t in times)))}
 
 
 # ---------------------------------------------------------------------------
@@ -314,6 +302,133 @@ def scaled_case(case, m):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def graph_region(eng, steps, ws):
+    """Steps replayed from a CUDA graph of two captured steps (launch gaps
+    removed), CUDA events on the graph's stream; returns (ms, steps timed)."""
+    import torch
+    from ftspolysol_b200.engine import Batch
+    b = Batch([eng], 2)
+    stream = torch.cuda.ExternalStream(b.stream())
+    b.step(1)
+    b.sync()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(steps // 2)
+    e1.record(stream)
+    b.sync()
+    barrier(ws)
+    b.close()
+    return e0.elapsed_time(e1), 2 * (steps // 2)
+
+
+def direct_region(eng, steps, ws, profile=False):
+    """Steps launched kernel by kernel (no step graph); with profile, every
+    propagator pass bracketed by CUDA events on the engine's stream."""
+    import torch
+    eng.set_step_graph(False)
+    if profile:
+        eng.profile(True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        eng.step_async()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    eng.set_step_graph(True)
+    return e0.elapsed_time(e1)
+
+
+def e2e_region(eng, om, ps, steps, ws):
+    """End to end through the public API: every step copies the fields in
+    from pinned host memory (ftsp_set_fields) and the record, Q and drift
+    maxima out (ftsp_step, which replays the engine's captured step graph)."""
+    import numpy as np
+    import torch
+    n_in = (eng.n_modes + 1) * eng.size
+    host = torch.empty(2 * n_in, dtype=torch.float64, pin_memory=True)
+    fields = np.concatenate([np.asarray(om).reshape(-1), np.asarray(ps).reshape(-1)])
+    host.numpy()[:] = fields.view(np.float64)
+    p_om = host.data_ptr()
+    p_ps = host.data_ptr() + eng.n_modes * eng.size * 16
+    ke = max(3, min(steps, 10))
+    eng.set_fields_ptr(p_om, p_ps)
+    eng.step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        eng.set_fields_ptr(p_om, p_ps)
+        eng.step()
+    t1 = time.perf_counter()
+    barrier(ws)
+    e_s = dist_max(t1 - t0, ws)
+    return {"value": ws * ke / e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * n_in,
+            "d2h_bytes_per_step": 16 * (eng.record_len + eng.n_species) + 8 * (eng.n_modes + 1),
+            "steps": ke, "api": "ftsp_set_fields + ftsp_step (host pinned fields in, record out)"}
+
+
+def cufft_segment(m, segments=49, reps=5):
+    """The reference's segment step on the library FFT (polymer.cu:396-400,
+    common.h:1079-1085): cuFFT forward C2C, one pointwise kernel (Phi/V), cuFFT
+    inverse C2C, one pointwise kernel (exp(-W)) writing the next stored
+    propagator; complex64, plans made once (torch.fft, which calls cuFFT),
+    replayed from a CUDA graph of `segments` segment steps."""
+    import torch
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev).manual_seed(5)
+    k = 2 * torch.pi * torch.fft.fftfreq(m, d=0.5, device=dev, dtype=torch.float64)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    phiV = (torch.exp(-k2 / 6.0) / m ** 3).to(torch.float32)
+    w = 0.1 * torch.randn((m, m, m), generator=g, device=dev, dtype=torch.float32)
+    E = torch.exp(-w).to(torch.complex64)
+    q = torch.ones((segments + 1, m, m, m), dtype=torch.complex64, device=dev)
+    X = torch.empty((m, m, m), dtype=torch.complex64, device=dev)
+    Y = torch.empty_like(X)
+
+    def sweep():
+        for s in range(segments):
+            torch.fft.fftn(q[s], out=X)
+            X.mul_(phiV)
+            torch.fft.ifftn(X, norm="forward", out=Y)
+            torch.mul(Y, E, out=q[s + 1])
+
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            sweep()
+    torch.cuda.current_stream().wait_stream(stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        sweep()
+    graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    us_graph = e0.elapsed_time(e1) * 1e3 / (reps * segments)
+    e0.record()
+    for _ in range(reps):
+        sweep()
+    e1.record()
+    torch.cuda.synchronize()
+    us_eager = e0.elapsed_time(e1) * 1e3 / (reps * segments)
+    del graph
+    return {"us_per_segment_graph": us_graph, "us_per_segment_eager": us_eager, "segments": segments,
+            "reps": reps, "grid": m, "dtype": "c64"}
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -336,56 +451,17 @@ def run_ours(args, ws, rank, local):
         eng.step_async()
     torch.cuda.synchronize()
 
-    def timed_region(profile: bool):
-        # kernels launched one by one (no step graph); with profile, every
-        # propagator pass bracketed by CUDA events
-        eng.set_step_graph(False)
-        if profile:
-            eng.profile(True)
-        barrier(ws)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
-            eng.step_async()
-        e1.record()
-        torch.cuda.synchronize()
-        barrier(ws)
-        eng.set_step_graph(True)
-        return e0.elapsed_time(e1)
-
-    def graph_region():
-        """The same steps replayed from a CUDA graph of two captured steps
-        (launch gaps removed); events on the graph's stream."""
-        from ftspolysol_b200.engine import Batch
-        b = Batch([eng], 2)
-        stream = torch.cuda.ExternalStream(b.stream())
-        b.step(1)
-        b.sync()
-        barrier(ws)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        b.step(args.steps // 2)
-        e1.record(stream)
-        b.sync()
-        barrier(ws)
-        b.close()
-        return e0.elapsed_time(e1), 2 * (args.steps // 2)
-
     # timed region for `value`: no instrumentation
     clocks = ClockSampler(local)
     clocks.start()
-    if args.no_graph or args.steps < 2:
-        ms = timed_region(False)
+    direct = args.no_graph or args.steps < 2
+    if direct:
+        ms = direct_region(eng, args.steps, ws)
         timed_steps = args.steps
     else:
-        ms, timed_steps = graph_region()
+        ms, timed_steps = graph_region(eng, args.steps, ws)
     ck = clocks.stop()
-    direct = args.no_graph or args.steps < 2
-    ms_direct = None if direct else timed_region(False)
+    ms_direct = None if direct else direct_region(eng, args.steps, ws)
     launches_per_step = eng.launches()
     status, rec, _ = eng.read_status()
     restarts = eng.restarts()
@@ -393,7 +469,7 @@ def run_ours(args, ws, rank, local):
     value = ws * timed_steps / (ms_max * 1e-3)
     # a second timed region of the same length with every propagator pass
     # bracketed by CUDA events on the engine's stream: per-kernel durations
-    ms_prof = timed_region(True)
+    ms_prof = direct_region(eng, args.steps, ws, profile=True)
     prof = eng.profile_read()
     eng.profile(False)
 
@@ -414,7 +490,7 @@ def run_ours(args, ws, rank, local):
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "traffic": traffic, "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
                 "timing": "per-kernel CUDA events over a second timed region of %d steps (%.2f ms/step with "
-                          "the events, %.2f ms/step without)" % (args.steps, ms_prof / args.steps, ms / args.steps),
+                          "the events, %.2f ms/step without)" % (args.steps, ms_prof / args.steps, ms / timed_steps),
                 "step": step_roofline(prop_bytes, field, args.steps, eng.size, 8 if prec == FP32 else 16,
                                       value / ws, peak),
                 "all_propagator_passes": {"achieved": prop_bytes / (prop_ms * 1e-3) / 1e9,
@@ -422,54 +498,46 @@ def run_ours(args, ws, rank, local):
                                           "per_kind": {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / v["launches"],
                                                            "GBps": v["bytes"] / v["ms"] * 1e-6}
                                                        for k, v in sorted(prof.items())}}}
+    seg_us = None
+    if "plane_fwd_mid" in prof and "bond_fwd" in prof:
+        seg_us = 1e3 * (prof["plane_fwd_mid"]["ms"] / prof["plane_fwd_mid"]["launches"]
+                        + prof["bond_fwd"]["ms"] / prof["bond_fwd"]["launches"])
 
-    # end to end through the public API: host fields in, record out, every step
-    e2e = None
-    if not args.no_e2e:
-        n_in = (eng.n_modes + 1) * eng.size
-        host = torch.empty(2 * n_in, dtype=torch.float64, pin_memory=True)
-        fields = np.concatenate([np.asarray(om).reshape(-1), np.asarray(ps).reshape(-1)])
-        host.numpy()[:] = fields.view(np.float64)
-        p_om = host.data_ptr()
-        p_ps = host.data_ptr() + eng.n_modes * eng.size * 16
-        ke = max(3, min(args.steps, 10))
-        eng.set_fields_ptr(p_om, p_ps)
-        eng.step()
-        torch.cuda.synchronize()
-        barrier(ws)
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            eng.set_fields_ptr(p_om, p_ps)
-            eng.step()
-        t1 = time.perf_counter()
-        barrier(ws)
-        e_s = dist_max(t1 - t0, ws)
-        e2e = {"value": ws * ke / e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * n_in,
-               "d2h_bytes_per_step": 16 * (eng.record_len + eng.n_species) + 8 * (eng.n_modes + 1),
-               "steps": ke, "api": "ftsp_set_fields + ftsp_step (host pinned fields in, record out)"}
+    e2e = None if args.no_e2e else e2e_region(eng, om, ps, args.steps, ws)
     eng.close()
 
     extra = {}
-    if rank == 0 and ws == 1 and not args.no_fp64_line and prec == FP32:
-        e64 = Engine(derived, precision=FP64, noise=True, seed=99, device=local, scheme=scheme,
+    if not args.no_fp64_line and prec == FP32:
+        # like for like with the reference build: complex128 throughout and the
+        # reference's predictor-corrector scheme, timed exactly as `value`
+        e64 = Engine(derived, precision=FP64, noise=True, seed=99 + rank, device=local, scheme=SCHEME_PC,
                      restart_interval=args.checkpoint_every)
         e64.set_fields(om, ps)
-        for _ in range(2):
+        for _ in range(args.warmup):
             e64.step_async()
         torch.cuda.synchronize()
-        k64 = max(3, args.steps // 4)
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record()
-        for _ in range(k64):
-            e64.step_async()
-        a1.record()
-        torch.cuda.synchronize()
+        if direct:
+            ms64, k64 = direct_region(e64, args.steps, ws), args.steps
+        else:
+            ms64, k64 = graph_region(e64, args.steps, ws)
         st64, _, _ = e64.read_status()
-        ms64 = a0.elapsed_time(a1)
-        extra["fp64"] = {"steps_per_s": k64 / (ms64 * 1e-3), "ms_per_step": ms64 / k64, "steps": k64,
-                         "status": int(st64), "dtype": "c128"}
+        ms64 = dist_max(ms64, ws)
+        block = {"value": ws * k64 / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64 / k64, "steps": k64,
+                 "warmup": args.warmup, "status": int(st64), "dtype": "c128",
+                 "scheme": "predictor-corrector (the reference's scheme)",
+                 "timed_as": "individual launches" if direct else "CUDA-graph replay of two captured steps"}
+        if not args.no_e2e:
+            block["e2e"] = e2e_region(e64, om, ps, args.steps, ws)
         e64.close()
+        extra["fp64_pc"] = block
+
+    if rank == 0 and ws == 1 and args.grid == 128 and not args.no_cufft:
+        cf = cufft_segment(128)
+        cf["ours_us_per_segment"] = seg_us
+        cf["ours"] = ("plane_fwd_mid + bond_fwd per-launch CUDA-event times (one forward segment step: inverse yz, "
+                      "exp(-W), store, forward yz; forward x, Phi/V, inverse x)")
+        cf["speedup_graph"] = (cf["us_per_segment_graph"] / seg_us) if seg_us else None
+        extra["cufft_segment_step"] = cf
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -506,7 +574,10 @@ def run_ours(args, ws, rank, local):
 # time to Pi: learned complex64 SI at dt = 0.02 against the plain runs
 # ---------------------------------------------------------------------------
 def _trajectory(eng, steps, t_wall0, rows, sim0, dt):
-    """Steps with a synchronous record each; rows get (wall s, sim time, Pi, mu)."""
+    """Steps with a synchronous record each; rows get (wall s, sim time, Pi,
+    mu).  A non-finite step is rolled back by the device on the next step
+    (at most max_restarts times); once the cap is reached the run is over
+    and the trajectory stops.  Returns (non-finite steps, stopped)."""
     import time
     from ftspolysol_b200.engine import NonFinite
     bad = 0
@@ -515,8 +586,10 @@ def _trajectory(eng, steps, t_wall0, rows, sim0, dt):
             _, rec, _ = eng.step()
             rows.append((time.perf_counter() - t_wall0, sim0 + (k + 1) * dt, rec[-1].real, rec[0].real))
         except NonFinite:
-            bad += 1   # the device rollback restores the last checkpoint on the next step
-    return bad
+            bad += 1
+            if eng.rollback_exhausted():
+                return bad, True
+    return bad, False
 
 
 def _time_to_target(rows, target, tol=0.01, every=50):
@@ -564,8 +637,9 @@ def run_time_to_pi(args, local):
         torch.cuda.synchronize()
         rows = []
         t0 = time.perf_counter()
-        bad = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt)
-        runs[tag] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "wall_s": rows[-1][0] if rows else None}
+        bad, stopped = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt)
+        runs[tag] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
+                     "wall_s": rows[-1][0] if rows else None}
         e.close()
 
     plain(FP64, 0.005, "c128_si_dt0.005")
@@ -585,7 +659,7 @@ def run_time_to_pi(args, local):
     t0 = time.perf_counter()
     ntrain = min(args.ttp_train_steps, int(round(T / 0.005)) // 2)
     e.learn_collect(True)
-    bad = _trajectory(e, ntrain, t0, rows, 0.0, 0.005)
+    bad, stopped = _trajectory(e, ntrain, t0, rows, 0.0, 0.005)
     loss = e.learn_train(1500)
     t_train = time.perf_counter() - t0
     e.set_dt(0.02)
@@ -594,14 +668,17 @@ def run_time_to_pi(args, local):
     sim = ntrain * 0.005
     nbig = int(round((T - sim) / 0.02))
     done = 0
-    while done < nbig:
+    while done < nbig and not stopped:
         k = min(200, nbig - done)
-        bad += _trajectory(e, k, t0, rows, sim + done * 0.02, 0.02)
+        b, stopped = _trajectory(e, k, t0, rows, sim + done * 0.02, 0.02)
+        bad += b
         done += k
-        e.learn_train(200)
-        e.learn_reset()
+        if not stopped:
+            e.learn_train(200)
+            e.learn_reset()
     st = e.learn_stats()
-    runs["c64_learned_dt0.02"] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "wall_s": rows[-1][0],
+    runs["c64_learned_dt0.02"] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
+                                  "wall_s": rows[-1][0] if rows else None,
                                   "train_steps": ntrain, "train_wall_s": t_train, "train_loss": loss,
                                   "fallback_steps": st["fallbacks"], "judged_steps": st["checks"]}
     e.close()

@@ -75,6 +75,7 @@ HostCfg make_cfg(const ftsp_config* in)
     c.scheme = in->scheme;
     c.device = in->device;
     c.restart_interval = in->restart_interval > 0 ? in->restart_interval : 0;
+    c.max_restarts = in->max_restarts > 0 ? in->max_restarts : 20;
     c.autotune = in->autotune != 0 ? 1 : 0;
     if (c.record_len() > 128) throw std::runtime_error("observable record too long");
     return c;
@@ -353,6 +354,16 @@ int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_len
     return FTSP_OK;
 }
 
+int ftsp_rollback_info(ftsp_handle* h, long long* restarts, int* exhausted)
+{
+    FTSP_GUARD(h, {
+        const long long r = h->eng->restarts();
+        if (restarts) *restarts = r;
+        if (exhausted) *exhausted = h->eng->restarts_exhausted() ? 1 : 0;
+    });
+    return FTSP_OK;
+}
+
 long long ftsp_restart_count(ftsp_handle* h)
 {
     if (!h || !h->eng) return -1;
@@ -553,23 +564,25 @@ void ftsp_batch_destroy(ftsp_batch* b)
 // ---------------------------------------------------------------------------
 // Chain propagation without any device allocation.
 //
-// For callers that cannot call cudaMalloc: code running while a CUDA stream
-// is being captured into a graph (allocation calls are not allowed there),
-// code inside a framework whose caching allocator owns the device memory
-// (e.g. a PyTorch process that has reserved the pool), and real-time loops
-// that must not block on the driver's allocator.  It computes exactly what
-// ftsp_propagate_chain computes, but all of its scratch lives in the single
-// file-scope array below, so no call allocates or frees device memory.
+// For callers that cannot call cudaMalloc: code inside a framework whose
+// caching allocator owns the device memory (e.g. a PyTorch process that has
+// reserved the pool), and real-time loops that must not block on the
+// driver's allocator.  It computes exactly what ftsp_propagate_chain
+// computes, but all of its scratch lives in the single file-scope array
+// below, so no call allocates or frees device memory.  The call is
+// synchronous: it copies its tables from host memory into the array, and
+// copies Q back to the host and waits for the stream before returning.
 //
 // Limits: at most NOALLOC_MAX_POINTS grid points (64^3) and NOALLOC_MAX_EXTENT
 // points along any axis; complex128 only.  The array (about 8.3 MiB) is part
 // of the library image, so every GPU that loads libftsp.so holds it until the
-// process exits.  Every call on a device shares it: calls whose work overlaps
-// on the GPU (different streams, or different host threads) race on it and
-// must be serialised by the caller.  Each call writes every part of the
-// scratch it later reads (the exp(-w) table, the intermediate field, the
-// reduction partials, the FFT and bond tables), so no region has to start at
-// zero and nothing carries over from the previous call.
+// process exits.  Every call on a device shares all of it, the tables
+// included: calls whose work overlaps on the GPU (different host threads on
+// different streams) race on it and must be serialised by the caller.  Each
+// call writes every part of the scratch it later reads (the exp(-w) table,
+// the intermediate field, the reduction partials, the FFT and bond tables),
+// so no region has to start at zero and nothing carries over from the
+// previous call.
 // ---------------------------------------------------------------------------
 namespace {
 

@@ -74,6 +74,7 @@ struct DevScal {
     alignas(16) int nonfinite;
     int bad_last;                          // the last step produced a non-finite value
     int restarts;                          // checkpoint rollbacks so far
+    int exhausted;                         // a non-finite step found max_restarts rollbacks taken: final
     int lr_use;                            // the next step preconditions with the learned G(k)
     int lr_checks;                         // steps judged by the residual test
     int lr_fallbacks;                      // of those, steps that fell back to the analytic G(k)
@@ -118,6 +119,7 @@ struct HostCfg {
     uint64_t seed;
     int precision, scheme, device;
     int restart_interval;   // device checkpoint every so many steps; rollback on a non-finite step (0: off)
+    int max_restarts;       // rollbacks before a non-finite step is final (the reference's max_nan_restarts)
     int autotune;           // time the launch-geometry alternatives at creation
     int n_stress() const { return __builtin_popcount(stress_mask); }
     bool stress_on() const { return stress_mask != 0 || iso; }
@@ -539,6 +541,7 @@ struct EngineBase {
     virtual void views(ftsp_views* v) = 0;
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
     virtual long long restarts() = 0;
+    virtual bool restarts_exhausted() = 0;
     virtual void set_dt(double dt) = 0;
     virtual void set_adaptive(double u_ref) = 0;
     virtual void set_chain_symmetry(bool on) = 0;
@@ -1107,6 +1110,7 @@ struct Engine : EngineBase {
         int batch = 4096, refresh_every = 100;
         uint64_t seed = 7;
         long long collected = 0, power_updates = 0, since_refresh = 0;
+        long long valid_targets = 0;   // (k, field) targets of the last training call
         int adam_t = 0;
         double last_loss = 0.0;
         Buf<float> A, B, Pw, Pp;      // statistics: <Re(du dw*)>, <|dw|^2> per field and k; spectral powers
@@ -1321,10 +1325,16 @@ struct Engine : EngineBase {
         if (lr.on_collect) {
             float* A = lr.A.p;
             float* B = lr.B.p;
+            // a step that runs away leaves non-finite values at some k: those
+            // contributions are skipped so that they cannot poison the sums
             foreach(Vn * nf, [=] __device__(size_t i) {
                 const V a = du[i], b = dw[i];
-                A[i] += (float)((double)a.x * b.x + (double)a.y * b.y);
-                B[i] += (float)((double)b.x * b.x + (double)b.y * b.y);
+                const double ca = (double)a.x * b.x + (double)a.y * b.y;
+                const double cb = (double)b.x * b.x + (double)b.y * b.y;
+                if (isfinite(ca) && isfinite(cb)) {
+                    A[i] += (float)ca;
+                    B[i] += (float)cb;
+                }
             });
             ++lr.collected;
         }
@@ -1373,8 +1383,8 @@ struct Engine : EngineBase {
             const V a = fk[i], b = fk[Vn + i];
             const float pa = have_w ? (float)((double)a.x * a.x + (double)a.y * a.y) * invV : 0.0f;
             const float pb = elec ? (float)((double)b.x * b.x + (double)b.y * b.y) * invV : 0.0f;
-            Pw[i] += alpha * (pa - Pw[i]);
-            Pp[i] += alpha * (pb - Pp[i]);
+            if (isfinite(pa)) Pw[i] += alpha * (pa - Pw[i]);
+            if (isfinite(pb)) Pp[i] += alpha * (pb - Pp[i]);
         });
         ++lr.power_updates;
     }
@@ -1430,8 +1440,9 @@ struct Engine : EngineBase {
             t = ok ? (float)log(a / (b * ga)) : 0.0f;
             m = ok ? 1.0f : 0.0f;
         };
-        if (!lr.trained) {
-            // output biases start at the mean target of each field
+        // valid targets per field (and their sum, for the initial output biases)
+        double h[2 * mlp::NOUT_MAX];
+        {
             double* tsum = reinterpret_cast<double*>(ds->kobs);
             reduce<2 * mlp::NOUT_MAX>(Vn, [=] __device__(size_t i, double* acc) {
                 for (int f = 0; f < nf; ++f) {
@@ -1441,9 +1452,16 @@ struct Engine : EngineBase {
                     acc[2 * f + 1] += (double)m;
                 }
             }, tsum);
-            double h[2 * mlp::NOUT_MAX];
             FTSP_CUDA(cudaMemcpyAsync(h, tsum, sizeof(h), cudaMemcpyDeviceToHost, stream));
             FTSP_CUDA(cudaStreamSynchronize(stream));
+        }
+        lr.valid_targets = 0;
+        for (int f = 0; f < nf; ++f) lr.valid_targets += (long long)h[2 * f + 1];
+        if (lr.valid_targets == 0)
+            throw std::runtime_error("ftsp_learn_train: no valid training target (every collected statistic is "
+                                     "non-finite or non-positive)");
+        if (!lr.trained) {
+            // output biases start at the mean target of each field
             std::vector<float> b3(nf);
             for (int f = 0; f < nf; ++f) b3[f] = h[2 * f + 1] > 0.0 ? (float)(h[2 * f] / h[2 * f + 1]) : 0.0f;
             FTSP_CUDA(cudaMemcpyAsync(lr.w.p + mlp::off_b3(nf), b3.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, stream));
@@ -1501,6 +1519,7 @@ struct Engine : EngineBase {
         st->iterations = lr.adam_t;
         st->using_learned = lr.on_use && hs.lr_use ? 1 : 0;
         st->n_params = lr.np;
+        st->valid_targets = lr.valid_targets;
     }
 
     int learn_weights(float* out, int n, bool set) override
@@ -2808,7 +2827,10 @@ struct Engine : EngineBase {
         } else {
             FTSP_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(V) * Vn, stream));
         }
+        // a new run: no pending rollback, no rollbacks taken
         FTSP_CUDA(cudaMemsetAsync(&ds->bad_last, 0, sizeof(int), stream));
+        FTSP_CUDA(cudaMemsetAsync(&ds->restarts, 0, sizeof(int), stream));
+        FTSP_CUDA(cudaMemsetAsync(&ds->exhausted, 0, sizeof(int), stream));
         if (c.restart_interval > 0) {
             if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(ck.p, omega.p, sizeof(V) * nm * Vn, cudaMemcpyDeviceToDevice, stream));
             FTSP_CUDA(cudaMemcpyAsync(ck.p + (size_t)nm * Vn, psi.p, sizeof(V) * Vn, cudaMemcpyDeviceToDevice, stream));
@@ -2862,6 +2884,20 @@ struct Engine : EngineBase {
             if (out) {
                 std::vector<float> tmp(nr);
                 FTSP_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * nr, cudaMemcpyDeviceToHost, stream));
+                FTSP_CUDA(cudaStreamSynchronize(stream));
+                for (size_t i = 0; i < nr; ++i) {
+                    out[2 * i] = (double)tmp[i];
+                    out[2 * i + 1] = 0.0;
+                }
+            }
+            return (long long)(2 * nr);
+        }
+        else if (name == "eta") {
+            // the last step's real noise, modes then psi (psi after its mean removal)
+            const size_t nr = (size_t)(nm + 1) * Vn;
+            if (out) {
+                std::vector<T> tmp(nr);
+                FTSP_CUDA(cudaMemcpyAsync(tmp.data(), eta.p, sizeof(T) * nr, cudaMemcpyDeviceToHost, stream));
                 FTSP_CUDA(cudaStreamSynchronize(stream));
                 for (size_t i = 0; i < nr; ++i) {
                     out[2 * i] = (double)tmp[i];
@@ -2970,8 +3006,13 @@ struct Engine : EngineBase {
     // ---- device-side checkpoint and rollback (complexLangevin.cu:583-636 semantics) ----
     // A step that ends with a non-finite field, Q or observable sets bad_last;
     // the next step first restores (omega, psi) from the last checkpoint and
-    // counts a restart.  Checkpoints are taken every restart_interval steps
-    // from a finite state.  Everything stays on the device.
+    // counts a restart.  Once max_restarts rollbacks have been taken, a
+    // further non-finite step is final (the reference stops with "maximum
+    // non-finite restarts exceeded", complexLangevin.cu:626-636): nothing is
+    // restored any more and the exhausted flag keeps every later step
+    // non-finite until set_fields starts a new run.  Checkpoints are taken
+    // every restart_interval steps from a finite state.  Everything stays on
+    // the device.
     void restore_if_bad()
     {
         const size_t Vn = V_;
@@ -2980,15 +3021,20 @@ struct Engine : EngineBase {
         V* ps = psi.p;
         const V* ckp = ck.p;
         DevScal* d = ds;
+        const int cap = c.max_restarts;
         foreach(Vn, [=] __device__(size_t i) {
-            if (!d->bad_last) return;
+            if (!d->bad_last || d->exhausted || d->restarts >= cap) return;
             for (int a = 0; a < nm; ++a) om[(size_t)a * Vn + i] = ckp[(size_t)a * Vn + i];
             ps[i] = ckp[(size_t)nm * Vn + i];
         });
         k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
-            if (d->bad_last) {
-                d->restarts += 1;
-                d->bad_last = 0;
+            if (d->bad_last && !d->exhausted) {
+                if (d->restarts >= cap) {
+                    d->exhausted = 1;
+                } else {
+                    d->restarts += 1;
+                    d->bad_last = 0;
+                }
             }
         });
         ++launches;
@@ -2999,7 +3045,7 @@ struct Engine : EngineBase {
         DevScal* d = ds;
         const int S = (int)c.sp.size(), R = c.record_len();
         k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
-            bool bad = d->nonfinite != 0 || d->corr[2] != 0.0;
+            bool bad = d->nonfinite != 0 || d->corr[2] != 0.0 || d->exhausted != 0;
             for (int s = 0; s < S; ++s) bad |= !(isfinite(d->Q[s].x) && isfinite(d->Q[s].y));
             for (int i = 0; i < 2 * R; ++i) bad |= !isfinite(d->rec[i]);
             d->bad_last = bad ? 1 : 0;
@@ -3151,7 +3197,7 @@ struct Engine : EngineBase {
             dmax[c.nm] = std::fabs(0.5 * c.lpsi) * std::sqrt(std::max(0.0, hs.dmax[c.nm]));
         }
         int st = status_from_host();
-        if (hs.corr[2] != 0.0) st = FTSP_NONFINITE;
+        if (hs.corr[2] != 0.0 || hs.exhausted) st = FTSP_NONFINITE;
         return st;
     }
 
@@ -3236,6 +3282,12 @@ struct Engine : EngineBase {
     {
         pull_scalars();
         return hs.restarts;
+    }
+
+    bool restarts_exhausted() override
+    {
+        pull_scalars();
+        return hs.exhausted != 0;
     }
 
     void views(ftsp_views* v) override

@@ -840,6 +840,7 @@ void fill_config(Model& m, ftsp_config& c)
 {
     const Param& p = m.p;
     std::memset(&c, 0, sizeof(c));
+    c.max_restarts = p.max_nan_restarts;
     c.m1 = p.m1;
     c.m2 = p.m2;
     c.m3 = p.m3;

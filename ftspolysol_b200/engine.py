@@ -48,6 +48,7 @@ class ftsp_config(C.Structure):
         ("self_pressure", C.c_double), ("stress_mask", C.c_int), ("isotropic_pressure", C.c_int),
         ("noise", C.c_int), ("seed", C.c_ulonglong), ("precision", C.c_int), ("scheme", C.c_int),
         ("device", C.c_int), ("restart_interval", C.c_int), ("autotune", C.c_int),
+        ("max_restarts", C.c_int),
     ]
 
 
@@ -75,7 +76,8 @@ class ftsp_learn_stats(C.Structure):
     _fields_ = [("collected", C.c_longlong), ("checks", C.c_longlong), ("fallbacks", C.c_longlong),
                 ("residual_learned", C.c_double), ("residual_analytic", C.c_double),
                 ("residual_learned_sum", C.c_double), ("residual_analytic_sum", C.c_double), ("loss", C.c_double),
-                ("iterations", C.c_int), ("using_learned", C.c_int), ("n_params", C.c_int)]
+                ("iterations", C.c_int), ("using_learned", C.c_int), ("n_params", C.c_int),
+                ("valid_targets", C.c_longlong)]
 
 
 _lib = None
@@ -116,6 +118,7 @@ def lib():
         L.ftsp_propagate_chain.argtypes = [vp, vp, C.c_int, C.c_double, vp, vp]
         L.ftsp_restart_count.restype = C.c_longlong
         L.ftsp_restart_count.argtypes = [vp]
+        L.ftsp_rollback_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
         L.ftsp_propagate_chain_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                                    vp, C.c_int, C.c_double, vp, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
@@ -155,7 +158,8 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
-               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_set_dt",
+               "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_rollback_info",
+               "ftsp_set_dt",
                "ftsp_tune_info_get", "ftsp_set_adaptive", "ftsp_step_info", "ftsp_set_chain_symmetry", "ftsp_set_step_graph",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
                "ftsp_learn_get_stats", "ftsp_learn_get_weights", "ftsp_learn_set_weights", "ftsp_learn_grad",
@@ -174,13 +178,13 @@ def _ip(a):
 def propagate_chain_noalloc(m, L, w_ptr: int, N: int, bond_length: float, q_end_ptr: int, stream: int = 0):
     """Chain propagation that allocates no device memory (no handle needed).
 
-    For callers that cannot allocate: inside CUDA stream capture, under a
-    framework that owns the device memory pool, or in loops that must not
-    wait on the allocator.  w and q_end are device pointers to m1*m2*m3
-    complex128 values; at most 64^3 points and 256 per axis.  Make the first
-    call on a device before any stream capture (it looks up the scratch
-    address), and do not run calls concurrently: they share one scratch
-    array.  Returns (status, Q)."""
+    For callers that cannot allocate: under a framework that owns the device
+    memory pool, or in loops that must not wait on the allocator.  w and
+    q_end are device pointers to m1*m2*m3 complex128 values; at most 64^3
+    points and 256 per axis.  The call is synchronous (it waits for the
+    stream and returns Q on the host).  Do not run calls concurrently from
+    several threads: they share one scratch array, tables included.
+    Returns (status, Q)."""
     Q = np.zeros(2)
     rc = lib().ftsp_propagate_chain_noalloc(int(m[0]), int(m[1]), int(m[2]), float(L[0]), float(L[1]), float(L[2]),
                                             C.c_void_p(w_ptr), int(N), float(bond_length), C.c_void_p(q_end_ptr),
@@ -204,7 +208,8 @@ class Engine:
     """
 
     def __init__(self, derived: dict, precision: int = FP64, scheme: int = SCHEME_PC, noise: bool = False,
-                 seed: int = 0, device: int = 0, restart_interval: int = 0, autotune: bool = False):
+                 seed: int = 0, device: int = 0, restart_interval: int = 0, autotune: bool = False,
+                 max_restarts: int = 20):
         L = lib()
         self._keep = []
 
@@ -264,6 +269,7 @@ class Engine:
         cfg.scheme = int(scheme)
         cfg.device = int(device)
         cfg.restart_interval = int(restart_interval)
+        cfg.max_restarts = int(max_restarts)
         cfg.autotune = int(bool(autotune))
         self.precision = precision
         self._cfg = cfg
@@ -454,6 +460,15 @@ class Engine:
 
     def restarts(self) -> int:
         return int(lib().ftsp_restart_count(self.h))
+
+    def rollback_exhausted(self) -> bool:
+        """True once a non-finite step found max_restarts rollbacks already
+        taken: the run is over (every later step is non-finite) until
+        set_fields starts a new one."""
+        r = C.c_longlong()
+        x = C.c_int()
+        self._check(lib().ftsp_rollback_info(self.h, C.byref(r), C.byref(x)), "rollback_info")
+        return bool(x.value)
 
     def launches(self) -> int:
         return int(lib().ftsp_last_launch_count(self.h))

@@ -84,6 +84,10 @@ typedef struct ftsp_config {
     int autotune;                /* 1: time the launch-geometry alternatives of the
                                     runtime-plan passes at creation (cached per
                                     grid in the process); no reference counterpart */
+    int max_restarts;            /* rollbacks allowed (restart_interval > 0) before a
+                                    non-finite step becomes final: the reference's
+                                    max_nan_restarts (param.h:74,
+                                    complexLangevin.cu:626-636); <= 0: 20       */
 } ftsp_config;
 
 typedef struct ftsp_handle ftsp_handle;
@@ -104,7 +108,9 @@ int ftsp_set_fields(ftsp_handle* h, const double* omega, const double* psi);
 /* Copies a named field to host memory as interleaved complex float64.
  * Names follow deviceState (deviceState.h:6-48): omega psi omega_bar psi_bar
  * drift drift_bar dpsi dpsi_bar rho_type rho_p rho_c rho_c_poly rho_c_ion
- * ion_rho W_type_s psi_s qF.  *count receives the number of doubles. */
+ * ion_rho W_type_s psi_s qF, and eta: the last step's real Langevin noise
+ * (modes, then psi after its mean removal; imaginary parts zero).  *count
+ * receives the number of doubles. */
 int ftsp_get_field(ftsp_handle* h, const char* name, double* out, long long* count);
 
 /* Densities at (omega, psi) (which = 0) or (omega_bar, psi_bar) (which = 1).
@@ -153,27 +159,39 @@ int ftsp_read_status(ftsp_handle* h, double* record, double* drift_max);
 int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_length, double* q_end, double* Q);
 
 /* ftsp_propagate_chain without any device allocation, for callers that
- * cannot call cudaMalloc: code that runs while a stream is being captured
- * into a CUDA graph, code inside a framework whose caching allocator owns the
- * device memory, real-time loops that must not block on the allocator.  No
- * counterpart in the reference.  No handle: the mesh (m1..m3) and box
- * lengths (L1..L3) are passed directly; w and q_end are device arrays of
- * m1*m2*m3 complex128 values, Q (host) receives mean(q_N).  All scratch lives
- * in one static device array of about 8.3 MiB inside the library, which every
- * GPU that loads libftsp.so keeps until the process exits.  Limits: at most
- * 262144 grid points (64^3) and 256 points per axis; larger meshes return
- * FTSP_ERROR with the reason in ftsp_last_error(NULL).  The first call on a
- * device looks the scratch address up with cudaGetSymbolAddress, so make that
- * first call before any stream capture begins.  Calls that overlap on the GPU
- * share the one scratch array and race: serialise them.  Runs on cuda_stream
- * (NULL: the legacy default stream) and returns after the stream has
- * finished the call's work. */
+ * cannot call cudaMalloc: code inside a framework whose caching allocator
+ * owns the device memory (a second allocator beside it fragments the pool or
+ * fails once the framework has reserved it), and loops that must not block
+ * on the driver's allocator.  No counterpart in the reference.  No handle:
+ * the mesh (m1..m3) and box lengths (L1..L3) are passed directly; w and
+ * q_end are device arrays of m1*m2*m3 complex128 values; Q points to 2 host
+ * doubles that receive mean(q_N) (real, imaginary).  All scratch (the
+ * exp(-w) table, the intermediate field, the reduction partials and the FFT
+ * and bond tables) lives in one static device array of about 8.3 MiB inside
+ * the library, which every GPU that loads libftsp.so keeps until the process
+ * exits.  Limits: at most 262144 grid points (64^3) and 256 points per axis;
+ * larger meshes return FTSP_ERROR with the reason in ftsp_last_error(NULL).
+ * The first call on a device looks the scratch address up with
+ * cudaGetSymbolAddress.  The call is synchronous: it copies its small tables
+ * from host memory into the array, runs on cuda_stream (NULL: the legacy
+ * default stream), copies Q back to the host and waits for the stream before
+ * returning.  Every call on a device shares the one array, tables included,
+ * so calls from different host threads whose work overlaps on the GPU race
+ * (even on tiny meshes): serialise them. */
 int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, double L3, const double* w, int N,
                                  double bond_length, double* q_end, double* Q, void* cuda_stream);
 
 /* Number of checkpoint rollbacks taken so far (restart_interval > 0);
  * -1 on error.  Synchronises the handle's stream. */
 long long ftsp_restart_count(ftsp_handle* h);
+
+/* Rollback state: *restarts as ftsp_restart_count; *exhausted = 1 once a
+ * non-finite step found max_restarts rollbacks already taken.  From then on
+ * nothing is restored and every step returns FTSP_NONFINITE, as the
+ * reference's run ends with "maximum non-finite restarts exceeded"
+ * (complexLangevin.cu:626-636), until ftsp_set_fields starts a new run
+ * (which clears both).  Synchronises the handle's stream. */
+int ftsp_rollback_info(ftsp_handle* h, long long* restarts, int* exhausted);
 
 /* Time step of the following steps (the noise amplitude, the predictor and
  * corrector coefficients and the semi-implicit P(k) follow it).  No
@@ -237,6 +255,9 @@ int ftsp_set_step_graph(ftsp_handle* h, int on);
  *                         backward and update kernels) regressing z_f on
  *                         log(<Re(du dw*)> / (<|dw|^2> G^Debye)); *loss
  *                         receives the last batch's mean squared error;
+ *                         the number of usable (finite, positive) targets
+ *                         is in ftsp_learn_stats.valid_targets, and with no
+ *                         usable target the call fails (FTSP_ERROR);
  *   ftsp_learn_use        while on, the SI update uses the learned G(k),
  *                         re-evaluated every refresh_every steps, except after
  *                         a step whose force residual sum_k |du - G dw|^2 with
@@ -262,6 +283,9 @@ typedef struct ftsp_learn_stats {
     int iterations;              /* Adam steps taken */
     int using_learned;           /* the next step uses the learned G(k) */
     int n_params;                /* network size in floats */
+    long long valid_targets;     /* (wave vector, field) targets the last ftsp_learn_train
+                                    could use: finite, positive statistics; with none
+                                    it fails with FTSP_ERROR */
 } ftsp_learn_stats;
 int ftsp_learn_configure(ftsp_handle* h, const ftsp_learn_config* cfg);
 int ftsp_learn_collect(ftsp_handle* h, int on);

@@ -30,7 +30,8 @@ void ftsp_model_free(ftsp_model* m);
 
 /* Fills an engine configuration from the model; its arrays point into the
  * model, which must outlive the config.  precision, scheme, seed, device and
- * restart_interval are left at zero for the caller to set. */
+ * restart_interval are left at zero for the caller to set; max_restarts is
+ * the param file's max_nan_restarts. */
 int ftsp_model_config(ftsp_model* m, ftsp_config* cfg);
 
 /* Scalar facts of a loaded model (no reference function; the reference

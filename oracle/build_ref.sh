@@ -8,10 +8,12 @@
 #   oracle/_ref/ref_harness  the reference's sources minus main.cu, linked with
 #                            oracle/ref_harness.cu (golden-vector dumps, timing)
 #
-# Usage: oracle/build_ref.sh [REFERENCE_DIR]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_DIR]
+#   REFERENCE_DIR defaults to $FTSP_REFERENCE_DIR, else to a directory named
+#   "reference" beside the repository.
 set -euo pipefail
-REF="${1:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${1:-${FTSP_REFERENCE_DIR:-$HERE/../../reference}}"
 OUT="$HERE/_ref"
 ARCH="-gencode arch=compute_100a,code=sm_100a"
 FLAGS="-O3 -std=c++17"

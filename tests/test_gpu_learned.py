@@ -98,7 +98,32 @@ def trained():
 def test_training_reduces_the_loss(trained):
     _, _, e, first, last = trained
     assert np.isfinite(last) and last < 0.5 * first
-    assert e.learn_stats()["iterations"] == 1500
+    st = e.learn_stats()
+    assert st["iterations"] == 1500
+    # (wave vector, field) targets with finite, positive statistics
+    assert 0.1 * 2 * 32 ** 3 < st["valid_targets"] <= 2 * 32 ** 3
+
+
+def test_training_needs_valid_targets():
+    """Statistics with no usable target (zero mobility and no noise: the
+    predictor never moves a field, so every <|dw|^2> is zero) make
+    ftsp_learn_train fail instead of returning the loss of an empty batch."""
+    from ftspolysol_b200.engine import FtspError
+    case = pe_case(16, N=8)
+    d = derive(case)
+    d = dict(d, lambda_psi=0.0, modes=[dict(m, **{"lambda": 0.0}) for m in d["modes"]])
+    e = Engine(d, precision=FP32, scheme=SCHEME_SI, noise=False)
+    om, ps = case.initial_fields()
+    e.set_fields(om, ps)
+    e.learn_configure(N=8, lB=1.0, salt=0.1, seed=3)
+    e.learn_collect(True)
+    for _ in range(3):
+        e.step_async()
+    e.learn_collect(False)
+    with pytest.raises(FtspError, match="no valid training target"):
+        e.learn_train(10)
+    assert e.learn_stats()["valid_targets"] == 0
+    e.close()
 
 
 def test_network_reproduces_the_measured_response(trained):

@@ -1,13 +1,14 @@
 """The allocation-free chain propagation against the allocating one.
 
 ftsp_propagate_chain_noalloc serves callers that cannot call cudaMalloc:
-code running while a stream is captured into a CUDA graph, code inside a
-framework whose caching allocator owns the device memory, and loops that must
-not wait on the allocator.  Its scratch is one static device array inside the
-library, so this test checks that two calls in a row (which reuse that array)
-each reproduce ftsp_propagate_chain, the handle-based entry point that
-allocates its scratch, to the FP64 tolerance of the other chain tests
-(1e-12 relative), and that meshes beyond the stated limit are refused.
+code inside a framework whose caching allocator owns the device memory, and
+loops that must not wait on the allocator.  Its scratch is one static device
+array inside the library, so this test checks that two calls in a row (which
+reuse that array) each reproduce ftsp_propagate_chain, the handle-based entry
+point that allocates its scratch, to the FP64 tolerance of the other chain
+tests (1e-12 relative), that the second call leaves the device's free memory
+unchanged (the driver's own count, so any allocation would show), and that
+meshes beyond the stated limit are refused.
 This file sorts last so that a run stopping at the first failure has already
 run every other test.
 """
@@ -38,9 +39,13 @@ def test_noalloc_matches_allocating_entry_point(m, N, b):
     eng.close()
     for call in range(2):
         q = torch.full_like(wd, complex("nan"))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         rc, Q = propagate_chain_noalloc(m, case.L, wd.data_ptr(), N, b, q.data_ptr())
         assert rc == 0, last_error()
         torch.cuda.synchronize()
+        if call == 1:   # the first call may load the library's kernels; a repeat call takes nothing
+            assert torch.cuda.mem_get_info()[0] == free0
         err_q = float((q - q_ref).abs().max() / q_ref.abs().max())
         assert err_q < TOL, (call, err_q)
         assert abs(Q - Q_ref) / abs(Q_ref) < TOL, (call, Q, Q_ref)
