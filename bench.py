@@ -63,6 +63,16 @@ def parse_args():
                     help="instead of the throughput line: this many independent replicas of uneven grids "
                          "(32^3-96^3), spread over the ranks and stepped as one CUDA graph per rank")
     ap.add_argument("--steps-per-graph", type=int, default=2)
+    ap.add_argument("--replica-seeds", type=int, default=1,
+                    help="replicas per system (seeds), for the ensemble statistics of --replicas")
+    ap.add_argument("--long-run", type=int, default=0,
+                    help="instead of the throughput line: this many steps of the 128^3 workload with device "
+                         "time averages of the record (Nss = 10, 10 blocks) and the capped rollback")
+    ap.add_argument("--long-precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--long-scheme", choices=["si", "pc"], default="si")
+    ap.add_argument("--long-dt", type=float, default=0.005)
+    ap.add_argument("--adaptive", type=float, default=0.0,
+                    help="adaptive step bound u_ref for --long-run (0: fixed step)")
     ap.add_argument("--precision-report", action="store_true",
                     help="instead of the throughput line: complex64 against complex128 on the 64^3, N = 50 "
                          "workload, per observable (mean and standard error over 10 blocks)")
@@ -706,6 +716,65 @@ def run_time_to_pi(args, local):
 
 
 # ---------------------------------------------------------------------------
+# long run: time-averaged observables of the 128^3 workload
+# ---------------------------------------------------------------------------
+def run_long(args, local):
+    """`--long-run K` steps of the 128^3 workload (seeded noise, full stress),
+    device time averages of the record (the reference's rule with Nss = 10,
+    complexLangevin.cu:424-467, plus 10 blocks for the errors), device
+    checkpoints every 10 steps and the capped rollback (20): the run stops when
+    the cap is reached, as the reference's does."""
+    import numpy as np
+    import torch
+    from ftspolysol_b200 import Engine, FP32, FP64, SCHEME_PC, SCHEME_SI
+    from ftspolysol_b200.cases import workload
+    from ftspolysol_b200.derive import derive
+
+    torch.cuda.set_device(local)
+    case = workload(4, noise=True, dt=args.long_dt)
+    if args.grid != 128:
+        case = scaled_case(case, args.grid)
+    d = derive(case)
+    prec = FP32 if args.long_precision == "fp32" else FP64
+    scheme = SCHEME_SI if args.long_scheme == "si" else SCHEME_PC
+    e = Engine(d, precision=prec, scheme=scheme, noise=True, seed=4321, device=local, restart_interval=10,
+               max_restarts=20)
+    om, ps = case.initial_fields()
+    e.set_fields(om, ps)
+    if args.adaptive > 0:
+        e.set_adaptive(args.adaptive)
+    K = args.long_run
+    e.average_start(case.Nss, K, 10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done, stopped = 0, False
+    while done < K and not stopped:
+        n = min(200, K - done)
+        for _ in range(n):
+            e.step_async()
+        done += n
+        stopped = e.rollback_exhausted()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    mean, se, cnt = e.average_read()
+    restarts = e.restarts()
+    e.close()
+    S, J = len(d["species"]), len(d["ions"])
+    names = (["mu_ex_poly"] + ["mu_ex_ion%d" % j for j in range(J)] + ["mu_self_%d" % i for i in range(S + J)] +
+             ["mu_id_%d" % i for i in range(S + J)] + ["H"] + ["stress_" + c for c in d["stress"]] + ["Pi"])
+    print(json.dumps({"metric": "time-averaged observables of the 128^3 N=50 workload", "steps_requested": K,
+                      "steps_taken": done, "records_averaged": cnt, "restarts": restarts, "stopped_at_cap": stopped,
+                      "wall_s": wall, "steps_per_s": done / wall,
+                      "config": {"workload": case.name + ": %d^3, L=%gb, N=50, divalent counterions, salt 0.05, "
+                                 "full stress + Pi, seeded noise" % (case.m[0], case.L[0]),
+                                 "precision": args.long_precision, "scheme": args.long_scheme, "dt": args.long_dt,
+                                 "adaptive_u_ref": args.adaptive or None, "Nss": case.Nss, "checkpoint_every": 10,
+                                 "max_restarts": 20},
+                      "averages": {n: {"mean": float(m), "se": float(s)} for n, m, s in zip(names, mean, se)}}))
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # replicas: many independent systems of uneven size, one CUDA graph per rank
 # ---------------------------------------------------------------------------
 def run_replicas(args, ws, rank, local):
@@ -717,7 +786,7 @@ def run_replicas(args, ws, rank, local):
     from ftspolysol_b200 import replicas as R
 
     torch.cuda.set_device(local)
-    cases_all = R.replica_set(args.replicas)
+    cases_all = R.replica_set(args.replicas, seeds_per_system=args.replica_seeds)
     mine = R.assign([R.cost(c) for c in cases_all], ws)[rank]
     engines = []
     for i in mine:
@@ -741,10 +810,16 @@ def run_replicas(args, ws, rank, local):
     a1.record()
     torch.cuda.synchronize()
     seq_ms = dist_max(a0.elapsed_time(a1), ws)
+    # time averages of every replica's record over the timed steps (device
+    # side, inside the graph): the batch warm-up steps are skipped
+    warm = max(1, args.warmup // args.steps_per_graph)
+    for e in engines:
+        e.average_start(warm * args.steps_per_graph, K * args.steps_per_graph,
+                        min(10, max(2, K * args.steps_per_graph // 4)))
     # one graph per rank: every replica on its own branch
     batch = Batch(engines, args.steps_per_graph)
     stream = torch.cuda.ExternalStream(batch.stream())
-    batch.step(max(1, args.warmup // args.steps_per_graph))
+    batch.step(warm)
     batch.sync()
     barrier(ws)
     torch.cuda.synchronize()
@@ -771,10 +846,18 @@ def run_replicas(args, ws, rank, local):
     results = {}
     for i, e in zip(mine, engines):
         st, rec, _ = e.read_status()
-        results[i] = {"status": int(st), "restarts": int(e.restarts()), "Pi": float(rec[-1].real) if len(rec) else None,
-                      "grid": cases_all[i].m[0], "N": len(cases_all[i].species[0].monomers)}
+        mean, se, cnt = e.average_read()
+        c = cases_all[i]
+        h = 3 * (e.n_species + e.n_ions)   # record: mu_ex, mu_self, mu_id, H, Pi
+        results[i] = {"status": int(st), "restarts": int(e.restarts()), "Pi_last": float(rec[-1].real),
+                      "grid": c.m[0], "N": len(c.species[0].monomers), "salt": c.salt["num_salt"] / c.volume,
+                      "records_averaged": cnt,
+                      "Pi": (float(mean[-1]), float(se[-1])), "H": (float(mean[h]), float(se[h])),
+                      "mu_ex": (float(mean[0]), float(se[0]))}
         e.close()
     results = R.gather(results, ws)
+    keys = {i: R.system_key(cases_all[i]) for i in results}
+    ens = R.ensemble(results, keys, ["Pi", "H", "mu_ex"])
     steps_done = dist_sum(len(mine) * K * args.steps_per_graph, ws)
     if rank == 0:
         by_grid = {}
@@ -797,7 +880,15 @@ def run_replicas(args, ws, rank, local):
             "graph_speedup": seq_ms / ms,
             "clocks": ck,
             "replicas_by_grid": by_grid,
-            "finite_replicas": sum(1 for r in results.values() if r["status"] == 0)}))
+            "finite_replicas": sum(1 for r in results.values() if r["status"] == 0),
+            "time_averages": {"rule": "records of the timed steps (the batch warm-up skipped), real parts, "
+                                      "standard error from block means; per system: mean over its seeds and "
+                                      "the standard error of that mean (a single seed keeps its block error)",
+                              "seeds_per_system": args.replica_seeds,
+                              "systems": {k: dict(v, **{"grid": results[min(i for i in results if keys[i] == k)]["grid"],
+                                                        "N": results[min(i for i in results if keys[i] == k)]["N"],
+                                                        "salt": results[min(i for i in results if keys[i] == k)]["salt"]})
+                                          for k, v in sorted(ens.items())}}}))
     return 0
 
 
@@ -879,6 +970,8 @@ def main():
             rc = run_replicas(args, ws, rank, local)
         elif args.time_to_pi:
             rc = run_time_to_pi(args, local) if rank == 0 else 0
+        elif args.long_run > 0:
+            rc = run_long(args, local) if rank == 0 else 0
         else:
             rc = run_ours(args, ws, rank, local)
     finally:

@@ -354,6 +354,20 @@ int ftsp_propagate_chain(ftsp_handle* h, const double* w, int N, double bond_len
     return FTSP_OK;
 }
 
+int ftsp_average_start(ftsp_handle* h, int skip, long long samples, int blocks)
+{
+    FTSP_GUARD(h, h->eng->average_start(skip, samples, blocks));
+    return FTSP_OK;
+}
+
+int ftsp_average_read(ftsp_handle* h, double* mean, double* std_error, long long* count)
+{
+    long long n = 0;
+    FTSP_GUARD(h, n = h->eng->average_read(mean, std_error));
+    if (count) *count = n;
+    return FTSP_OK;
+}
+
 int ftsp_rollback_info(ftsp_handle* h, long long* restarts, int* exhausted)
 {
     FTSP_GUARD(h, {

@@ -67,6 +67,8 @@ struct DevScal {
     alignas(16) double dmax[MAXMODE + 1];
     alignas(16) double rec[2 * 128];
     alignas(16) unsigned long long step;   // steps taken: keys the noise, schedules the checkpoints
+    long long avg_seen;                    // time averaging: steps since ftsp_average_start
+    long long avg_count;                   // of those, records accumulated
     alignas(16) double dt_scale;           // this step's dt / configured dt (1 unless the step is adaptive)
     double umax;                           // max |drift| at the start of this step (adaptive step)
     alignas(16) double lres[2];            // learned preconditioner: force residuals (learned, analytic) of the step
@@ -218,6 +220,33 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
 
 // Fixed-order combine of `count` partial rows of K channels: one warp per
 // channel (grid K), lanes stride over the rows, then a shuffle tree.
+// Time averaging of the observable record (complexLangevin.cu:424-441): a
+// step's record is accumulated when more than `skip` steps have been seen
+// since the averaging started, fewer than `samples` records have been
+// accumulated and the step is finite; the real part of every entry, weighted
+// by the step's dt scale (1 unless the step is adaptive), into block
+// avg_count / per_block.  acc holds per block R weighted sums, the weight sum
+// and the record count.  One CTA; the counters move after every thread has
+// read them.
+static __global__ void k_average(DevScal* d, double* acc, int R, long long skip, long long samples, long long per_block)
+{
+    const bool take = d->avg_seen + 1 > skip && d->avg_count < samples && !d->bad_last;
+    if (take) {
+        double* a = acc + (size_t)(d->avg_count / per_block) * (R + 2);
+        const double w = d->dt_scale;
+        for (int i = threadIdx.x; i < R; i += blockDim.x) a[i] += w * d->rec[2 * i];
+        if (threadIdx.x == 0) {
+            a[R] += w;
+            a[R + 1] += 1.0;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d->avg_seen += 1;
+        if (take) d->avg_count += 1;
+    }
+}
+
 template <bool MAX>
 __global__ void k_combine(const double* partial, int count, int K, double* out)
 {
@@ -542,6 +571,8 @@ struct EngineBase {
     virtual void propagate_chain(const double2* w, int N, double bond, double2* q_end, double* Q) = 0;
     virtual long long restarts() = 0;
     virtual bool restarts_exhausted() = 0;
+    virtual void average_start(long long skip, long long samples, int blocks) = 0;
+    virtual long long average_read(double* mean, double* std_error) = 0;
     virtual void set_dt(double dt) = 0;
     virtual void set_adaptive(double u_ref) = 0;
     virtual void set_chain_symmetry(bool on) = 0;
@@ -666,6 +697,7 @@ struct Engine : EngineBase {
         part.release(); spart.release(); stage.release(); expo.release(); pmax.release();
         pair_ix.release(); pair_wt.release(); pair_run.release();
         si_G.release(); si_inc.release(); ck.release();
+        avg.acc.release();
         learn_release();
         if (ds) cudaFree(ds);
         release_events();
@@ -3101,7 +3133,81 @@ struct Engine : EngineBase {
         corrector();
         if (learn) learn_after_step();
         mark_step_status();
+        if (avg.on) {
+            k_average<<<1, 128, 0, stream>>>(ds, avg.acc.p, c.record_len(), avg.skip, avg.samples, avg.per_block);
+            ++launches;
+        }
         if (c.restart_interval > 0) checkpoint_if_good();
+    }
+
+    // ---- time averages of the record (complexLangevin.cu:424-467) ----
+    struct Avg {
+        bool on = false;
+        long long skip = 0, samples = 0, per_block = 1;
+        int blocks = 0;
+        Buf<double> acc;
+    } avg;
+
+    void average_start(long long skip, long long samples, int blocks) override
+    {
+        if (skip < 0 || samples < 1) throw std::runtime_error("ftsp_average_start: need skip >= 0 and samples >= 1");
+        if (blocks < 1 || blocks > 1000 || blocks > samples)
+            throw std::runtime_error("ftsp_average_start: blocks must be in 1..min(samples, 1000)");
+        drop_step_graph();
+        avg.acc.release();
+        avg.skip = skip;
+        avg.samples = samples;
+        avg.blocks = blocks;
+        avg.per_block = (samples + blocks - 1) / blocks;
+        const int R = c.record_len();
+        const int nblk = (int)((samples + avg.per_block - 1) / avg.per_block);
+        avg.acc.alloc((size_t)nblk * (R + 2));
+        FTSP_CUDA(cudaMemsetAsync(avg.acc.p, 0, sizeof(double) * avg.acc.n, stream));
+        FTSP_CUDA(cudaMemsetAsync(&ds->avg_seen, 0, 2 * sizeof(long long), stream));
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+        avg.on = true;
+    }
+
+    // mean over every accumulated record (weighted by dt scale) and the
+    // standard error from the means of the complete blocks (NaN with fewer
+    // than two); returns the number of records accumulated
+    long long average_read(double* mean, double* se) override
+    {
+        if (!avg.on) throw std::runtime_error("ftsp_average_read: averaging was not started");
+        const int R = c.record_len();
+        std::vector<double> a(avg.acc.n);
+        FTSP_CUDA(cudaMemcpyAsync(a.data(), avg.acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, stream));
+        pull_scalars();
+        const int nblk = (int)(a.size() / (R + 2));
+        std::vector<double> sum(R, 0.0);
+        double wsum = 0.0;
+        std::vector<std::vector<double>> bm;
+        for (int b = 0; b < nblk; ++b) {
+            const double* x = a.data() + (size_t)b * (R + 2);
+            for (int i = 0; i < R; ++i) sum[i] += x[i];
+            wsum += x[R];
+            if (x[R + 1] >= (double)avg.per_block && x[R] > 0.0) {
+                std::vector<double> m(R);
+                for (int i = 0; i < R; ++i) m[i] = x[i] / x[R];
+                bm.push_back(m);
+            }
+        }
+        for (int i = 0; i < R; ++i) {
+            if (mean) mean[i] = wsum > 0.0 ? sum[i] / wsum : NAN;
+            if (se) {
+                if (bm.size() < 2) {
+                    se[i] = NAN;
+                    continue;
+                }
+                double mu = 0.0;
+                for (auto& m : bm) mu += m[i];
+                mu /= (double)bm.size();
+                double v = 0.0;
+                for (auto& m : bm) v += (m[i] - mu) * (m[i] - mu);
+                se[i] = std::sqrt(v / (double)(bm.size() - 1) / (double)bm.size());
+            }
+        }
+        return hs.avg_count;
     }
 
     int status_from_host()

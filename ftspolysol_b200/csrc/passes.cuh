@@ -393,6 +393,8 @@ struct OpProp {
     static constexpr bool FWD = KIND <= FWD_SINGLE;
     static constexpr bool NEED_E = KIND == FWD_START || KIND == FWD_MID || KIND == FWD_LAST || KIND == FWD_SINGLE ||
                                    KIND == BWD_START || KIND == BWD_MID;
+    // global loads per point (the forward passes read only the class table)
+    static constexpr int LOADS = FWD ? 1 : 4;
     static constexpr bool MAX_OUT = KIND == FWD_START || KIND == FWD_MID || KIND == BWD_START || KIND == BWD_MID;
     struct Pre {
         V e, q, r, c;
@@ -718,8 +720,12 @@ __global__ void __launch_bounds__(NT, 1) k_plane_fused(const cplx<T>* src, cplx<
     const int f = blockIdx.y;
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
-    pdl_wait();
+    // the L2 prefetch of the pointwise operands goes out before the wait for
+    // the previous pass: a prefetch only moves lines into L2, the device's
+    // point of coherence, so it cannot observe a stale value, and the class
+    // table (the bulk of it) is not written during a sweep
     if (threadIdx.x == 0) op.prefetch(base, (unsigned)NE);
+    pdl_wait();
     V v[E];   // value u: row tid/N + u*NT/N, column tid%N
 #pragma unroll
     for (int u = 0; u < E; ++u) v[u] = src[base + threadIdx.x + u * NT];
@@ -738,7 +744,9 @@ __global__ void __launch_bounds__(NT, 1) k_plane_fused(const cplx<T>* src, cplx<
     ct_fft<V, S1, N, RMAX, N, 1, P, NT, E>(tile, stw);                  // z-lines
     op.begin();
     constexpr int EPT = NE / NT;
-    constexpr int PB = (sizeof(T) == 4 && NT < 1024) ? 8 : 4;
+    // loads in flight per batch: every FFT value is in shared memory here,
+    // so the registers hold the operands of PB points
+    constexpr int PB = (sizeof(T) == 4 && Op::LOADS <= 1) ? 16 : 4;
 #pragma unroll 1
     for (int u0 = 0; u0 < EPT; u0 += PB) {
         typename Op::Pre pre[PB];

@@ -119,6 +119,8 @@ def lib():
         L.ftsp_restart_count.restype = C.c_longlong
         L.ftsp_restart_count.argtypes = [vp]
         L.ftsp_rollback_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
+        L.ftsp_average_start.argtypes = [vp, C.c_int, C.c_longlong, C.c_int]
+        L.ftsp_average_read.argtypes = [vp, vp, vp, C.POINTER(C.c_longlong)]
         L.ftsp_propagate_chain_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                                    vp, C.c_int, C.c_double, vp, vp, vp]
         L.ftsp_profile_enable.argtypes = [vp, C.c_int]
@@ -159,6 +161,7 @@ ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_strea
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
                "ftsp_propagate_chain", "ftsp_propagate_chain_noalloc", "ftsp_restart_count", "ftsp_rollback_info",
+               "ftsp_average_start", "ftsp_average_read",
                "ftsp_set_dt",
                "ftsp_tune_info_get", "ftsp_set_adaptive", "ftsp_step_info", "ftsp_set_chain_symmetry", "ftsp_set_step_graph",
                "ftsp_learn_configure", "ftsp_learn_collect", "ftsp_learn_reset", "ftsp_learn_train", "ftsp_learn_use",
@@ -460,6 +463,20 @@ class Engine:
 
     def restarts(self) -> int:
         return int(lib().ftsp_restart_count(self.h))
+
+    def average_start(self, skip: int, samples: int, blocks: int = 10):
+        """Starts device-side time averaging of the record: steps after the
+        first `skip`, at most `samples` finite records, in `blocks` blocks."""
+        self._check(lib().ftsp_average_start(self.h, int(skip), int(samples), int(blocks)), "average_start")
+
+    def average_read(self):
+        """(mean, standard error, records accumulated): real parts of the
+        record entries, the error from the block means."""
+        mean = np.zeros(self.record_len)
+        se = np.zeros(self.record_len)
+        n = C.c_longlong()
+        self._check(lib().ftsp_average_read(self.h, mean.ctypes.data, se.ctypes.data, C.byref(n)), "average_read")
+        return mean, se, int(n.value)
 
     def rollback_exhausted(self) -> bool:
         """True once a non-finite step found max_restarts rollbacks already

@@ -185,6 +185,24 @@ int ftsp_propagate_chain_noalloc(int m1, int m2, int m3, double L1, double L2, d
  * -1 on error.  Synchronises the handle's stream. */
 long long ftsp_restart_count(ftsp_handle* h);
 
+/* Time averages of the observable record on the device, following
+ * complexLangevin::accumulate_observable_record / write_observable_average
+ * (complexLangevin.cu:424-467): after ftsp_average_start, the record of a
+ * step is accumulated when more than `skip` steps (the reference's Nss) have
+ * been taken since the start, fewer than `samples` (Ns) records have been
+ * accumulated and the step is finite; the real part of every entry, as the
+ * reference averages and writes it.  With the adaptive step each record is
+ * weighted by its dt_eff / dt.  The records are also grouped into `blocks`
+ * consecutive blocks (no reference counterpart): ftsp_average_read returns
+ * the mean over all accumulated records (mean[ftsp_record_length]), the
+ * standard error from the means of the complete blocks (std_error[...],
+ * NaN with fewer than two complete blocks) and the number of records
+ * accumulated (*count).  Nothing is copied to the host during the steps, so
+ * averaging runs inside the step graph and replica batches; start it before
+ * ftsp_batch_create.  ftsp_average_start restarts the accumulation. */
+int ftsp_average_start(ftsp_handle* h, int skip, long long samples, int blocks);
+int ftsp_average_read(ftsp_handle* h, double* mean, double* std_error, long long* count);
+
 /* Rollback state: *restarts as ftsp_restart_count; *exhausted = 1 once a
  * non-finite step found max_restarts rollbacks already taken.  From then on
  * nothing is restored and every step returns FTSP_NONFINITE, as the

@@ -43,6 +43,25 @@ def test_assign_covers_every_replica_once_and_balances(ws):
     assert parts == R.assign(costs, ws)   # deterministic
 
 
+def test_ensemble_statistics():
+    """Mean and standard error over the seeds of one system; a system with a
+    single replica keeps its own time average and block error."""
+    cs = R.replica_set(8, seeds_per_system=2)
+    keys = {i: R.system_key(c) for i, c in enumerate(cs)}
+    assert len(set(keys.values())) == 4
+    for i in range(0, 8, 2):
+        assert keys[i] == keys[i + 1] and cs[i].init_seed != cs[i + 1].init_seed
+    res = {i: {"Pi": (1.0 + i, 0.1)} for i in range(8)}
+    res[8] = {"Pi": (7.0, 0.25)}
+    keys[8] = "single"
+    ens = R.ensemble(res, keys, ["Pi"])
+    g = ens[keys[0]]
+    assert g["replicas"] == 2
+    assert g["Pi"][0] == pytest.approx(1.5)
+    assert g["Pi"][1] == pytest.approx(0.5)       # std([1, 2], ddof=1) / sqrt(2)
+    assert ens["single"] == {"replicas": 1, "Pi": (7.0, 0.25)}
+
+
 WORKER = r"""
 import json, os, sys
 sys.path.insert(0, {root!r})
@@ -51,8 +70,10 @@ from ftspolysol_b200 import replicas as R
 ws, rank, local = bench.dist_setup()
 costs = [R.cost(c) for c in R.replica_set(16)]
 mine = R.assign(costs, ws)[rank]
-res = R.gather({{i: {{"rank": rank}} for i in mine}}, ws)
-out = {{"rank": rank, "mine": mine, "gathered": {{str(k): v for k, v in res.items()}},
+res = R.gather({{i: {{"rank": rank, "Pi": (float(i), 0.0)}} for i in mine}}, ws)
+cs = R.replica_set(16, seeds_per_system=2)
+ens = R.ensemble(res, {{i: R.system_key(c) for i, c in enumerate(cs)}}, ["Pi"])
+out = {{"rank": rank, "mine": mine, "gathered": {{str(k): v for k, v in res.items()}}, "ensemble": ens,
         "max": bench.dist_max(1.5 + rank, ws), "sum": bench.dist_sum(len(mine), ws)}}
 bench.barrier(ws)
 import torch.distributed as dist
@@ -88,4 +109,9 @@ def test_two_gloo_ranks():
     for k, v in a["gathered"].items():
         assert int(k) in (a["mine"] if v["rank"] == 0 else b["mine"])
     assert a["max"] == b["max"] == 2.5
+    # the ensemble over the gathered replicas: both ranks agree, and each
+    # system averages the indices of its two seeds (2j, 2j + 1)
+    assert a["ensemble"] == b["ensemble"] and len(a["ensemble"]) == 8
+    for g in a["ensemble"].values():
+        assert g["replicas"] == 2 and (g["Pi"][0] - 0.5) % 2 == 0
     assert a["sum"] == b["sum"] == 16
