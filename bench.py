@@ -57,6 +57,11 @@ def parse_args():
                     help="instead of the throughput line: time for Pi and mu to reach 1%% of the complex128 "
                          "semi-implicit dt=0.005 result, learned complex64 at dt=0.02 against plain runs")
     ap.add_argument("--ttp-time", type=float, default=20.0, help="simulated time of each time-to-Pi run")
+    ap.add_argument("--ttp-case", choices=["w5", "w2"], default="w5",
+                    help="time-to-Pi workload: w5 = the 128^3 divalent system (scaled by --grid), "
+                         "w2 = the 64^3 N=50 monovalent system")
+    ap.add_argument("--ttp-dts", type=lambda x: [float(v) for v in x.split(",")], default=[0.01, 0.02],
+                    help="step sizes of the complex64 plain and learned runs (comma separated)")
     ap.add_argument("--ttp-train-steps", type=int, default=2000,
                     help="plain semi-implicit steps whose statistics train the network")
     ap.add_argument("--replicas", type=int, default=0,
@@ -71,6 +76,8 @@ def parse_args():
     ap.add_argument("--long-precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--long-scheme", choices=["si", "pc"], default="si")
     ap.add_argument("--long-dt", type=float, default=0.005)
+    ap.add_argument("--max-restarts", type=int, default=20,
+                    help="rollbacks before a non-finite step ends a --long-run (the reference's max_nan_restarts)")
     ap.add_argument("--adaptive", type=float, default=0.0,
                     help="adaptive step bound u_ref for --long-run (0: fixed step)")
     ap.add_argument("--precision-report", action="store_true",
@@ -583,18 +590,22 @@ def run_ours(args, ws, rank, local):
 # ---------------------------------------------------------------------------
 # time to Pi: learned complex64 SI at dt = 0.02 against the plain runs
 # ---------------------------------------------------------------------------
-def _trajectory(eng, steps, t_wall0, rows, sim0, dt):
+def _trajectory(eng, steps, t_wall0, rows, sim0, dt, idx):
     """Steps with a synchronous record each; rows get (wall s, sim time, Pi,
-    mu).  A non-finite step is rolled back by the device on the next step
-    (at most max_restarts times); once the cap is reached the run is over
-    and the trajectory stops.  Returns (non-finite steps, stopped)."""
+    mu, mu_ex), mu being the polymer's total chemical potential
+    mu_ex + mu_self + mu_id (record entries idx).  A non-finite step is
+    rolled back by the device on the next step (at most max_restarts times);
+    once the cap is reached the run is over and the trajectory stops.
+    Returns (non-finite steps, stopped)."""
     import time
     from ftspolysol_b200.engine import NonFinite
     bad = 0
     for k in range(steps):
         try:
             _, rec, _ = eng.step()
-            rows.append((time.perf_counter() - t_wall0, sim0 + (k + 1) * dt, rec[-1].real, rec[0].real))
+            r = rec.real
+            rows.append((time.perf_counter() - t_wall0, sim0 + (k + 1) * dt, r[-1], r[idx[0]] + r[idx[1]] + r[idx[2]],
+                         r[idx[0]]))
         except NonFinite:
             bad += 1
             if eng.rollback_exhausted():
@@ -605,7 +616,7 @@ def _trajectory(eng, steps, t_wall0, rows, sim0, dt):
 def _time_to_target(rows, target, tol=0.01, every=50):
     """Earliest wall time from which on every running estimate (mean of Pi
     and mu over the second half of the trajectory so far, checked every
-    `every` steps) stays within tol of target."""
+    `every` steps) stays within tol (relative) of target."""
     import numpy as np
     a = np.array(rows)
     checks = []
@@ -622,6 +633,13 @@ def _time_to_target(rows, target, tol=0.01, every=50):
 
 
 def run_time_to_pi(args, local):
+    """Wall time for the running means of Pi and mu to settle within 1 % of
+    the complex128 semi-implicit dt = 0.005 result: complex128 and complex64
+    plain semi-implicit runs, and complex64 runs with the learned
+    preconditioner at larger steps (trained on the force/increment
+    statistics of plain dt = 0.005 steps, retrained online).  Every run
+    covers the same simulated time; the target is the second-half mean of
+    the complex128 run."""
     import time
     import numpy as np
     import torch
@@ -630,10 +648,15 @@ def run_time_to_pi(args, local):
     from ftspolysol_b200.derive import derive
 
     torch.cuda.set_device(local)
-    case = workload(5, noise=True)
-    if args.grid != 128:
-        case = scaled_case(case, args.grid)
+    if args.ttp_case == "w2":
+        case = workload(2, noise=True)
+    else:
+        case = workload(5, noise=True)
+        if args.grid != 128:
+            case = scaled_case(case, args.grid)
     d = derive(case)
+    S, J = len(d["species"]), len(d["ions"])
+    idx = (0, S + J, 2 * (S + J))   # mu_ex, mu_self, mu_id of the polymer
     om, ps = case.initial_fields()
     T = args.ttp_time
     salt = case.salt["num_salt"] / case.volume if case.salt else 0.0
@@ -647,70 +670,95 @@ def run_time_to_pi(args, local):
         torch.cuda.synchronize()
         rows = []
         t0 = time.perf_counter()
-        bad, stopped = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt)
-        runs[tag] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
-                     "wall_s": rows[-1][0] if rows else None}
+        bad, stopped = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt, idx)
+        runs[tag] = {"rows": rows, "dt": dt, "nonfinite_steps": bad, "restarts": e.restarts(),
+                     "stopped_at_cap": stopped, "wall_s": rows[-1][0] if rows else None}
+        e.close()
+
+    def learned(dt, tag):
+        # plain SI steps at dt = 0.005 collect the statistics, Adam trains the
+        # network, then steps of dt with the learned kernel, retrained online
+        e = Engine(dict(d, dt=0.005), precision=FP32, scheme=SCHEME_SI, noise=True, seed=21, device=local,
+                   restart_interval=20)
+        e.set_fields(om, ps)
+        e.learn_configure(N=N, lB=case.lB, salt=salt, seed=11)
+        torch.cuda.synchronize()
+        rows = []
+        t0 = time.perf_counter()
+        ntrain = min(args.ttp_train_steps, int(round(T / 0.005)) // 2)
+        e.learn_collect(True)
+        bad, stopped = _trajectory(e, ntrain, t0, rows, 0.0, 0.005, idx)
+        loss = e.learn_train(1500) if not stopped else None
+        valid = e.learn_stats()["valid_targets"]
+        t_train = time.perf_counter() - t0
+        if not stopped:
+            e.set_dt(dt)
+            e.learn_use(True)
+            e.learn_reset()
+        sim = ntrain * 0.005
+        nbig = int(round((T - sim) / dt))
+        done = 0
+        while done < nbig and not stopped:
+            k = min(200, nbig - done)
+            b, stopped = _trajectory(e, k, t0, rows, sim + done * dt, dt, idx)
+            bad += b
+            done += k
+            if not stopped:
+                e.learn_train(200)
+                e.learn_reset()
+        st = e.learn_stats()
+        runs[tag] = {"rows": rows, "dt": dt, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
+                     "wall_s": rows[-1][0] if rows else None, "train_steps": ntrain, "train_wall_s": t_train,
+                     "train_loss": loss, "valid_targets": valid, "fallback_steps": st["fallbacks"],
+                     "judged_steps": st["checks"]}
         e.close()
 
     plain(FP64, 0.005, "c128_si_dt0.005")
-    half = np.array(runs["c128_si_dt0.005"]["rows"])
-    half = half[len(half) // 2:]
-    target = (float(half[:, 2].mean()), float(half[:, 3].mean()))
+    base_rows = np.array(runs["c128_si_dt0.005"]["rows"])
+    half = base_rows[len(base_rows) // 2:]
+    target = (float(half[:, 2].mean()), float(half[:, 3].mean()), float(half[:, 4].mean()))
+    bm = np.array([b.mean(axis=0) for b in np.array_split(half[:, 2:5], 10)])
+    target_se = bm.std(axis=0, ddof=1) / np.sqrt(len(bm))
     plain(FP32, 0.005, "c64_si_dt0.005")
-    plain(FP32, 0.02, "c64_si_dt0.02")
-
-    # learned: plain SI steps at dt = 0.005 collect the statistics, Adam trains
-    # the network, then dt = 0.02 with the learned kernel, retrained online
-    e = Engine(dict(d, dt=0.005), precision=FP32, scheme=SCHEME_SI, noise=True, seed=21, device=local, restart_interval=20)
-    e.set_fields(om, ps)
-    e.learn_configure(N=N, lB=case.lB, salt=salt, seed=11)
-    torch.cuda.synchronize()
-    rows = []
-    t0 = time.perf_counter()
-    ntrain = min(args.ttp_train_steps, int(round(T / 0.005)) // 2)
-    e.learn_collect(True)
-    bad, stopped = _trajectory(e, ntrain, t0, rows, 0.0, 0.005)
-    loss = e.learn_train(1500)
-    t_train = time.perf_counter() - t0
-    e.set_dt(0.02)
-    e.learn_use(True)
-    e.learn_reset()
-    sim = ntrain * 0.005
-    nbig = int(round((T - sim) / 0.02))
-    done = 0
-    while done < nbig and not stopped:
-        k = min(200, nbig - done)
-        b, stopped = _trajectory(e, k, t0, rows, sim + done * 0.02, 0.02)
-        bad += b
-        done += k
-        if not stopped:
-            e.learn_train(200)
-            e.learn_reset()
-    st = e.learn_stats()
-    runs["c64_learned_dt0.02"] = {"rows": rows, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
-                                  "wall_s": rows[-1][0] if rows else None,
-                                  "train_steps": ntrain, "train_wall_s": t_train, "train_loss": loss,
-                                  "fallback_steps": st["fallbacks"], "judged_steps": st["checks"]}
-    e.close()
+    for dt in args.ttp_dts:
+        plain(FP32, dt, "c64_si_dt%g" % dt)
+        learned(dt, "c64_learned_dt%g" % dt)
 
     out = {}
     for tag, r in runs.items():
         a = np.array(r["rows"])
-        h = a[len(a) // 2:]
         info = {k: v for k, v in r.items() if k != "rows"}
-        info.update({"steps": len(a), "Pi_mean": float(h[:, 2].mean()), "mu_mean": float(h[:, 3].mean()),
-                     "Pi_rel_err": float(h[:, 2].mean() / target[0] - 1.0),
-                     "mu_rel_err": float(h[:, 3].mean() / target[1] - 1.0),
-                     "time_to_1pct_s": _time_to_target(r["rows"], target)})
+        if len(a) >= 2:
+            h = a[len(a) // 2:]
+            info.update({"steps": len(a), "Pi_mean": float(h[:, 2].mean()), "mu_mean": float(h[:, 3].mean()),
+                         "mu_ex_mean": float(h[:, 4].mean()),
+                         "Pi_rel_err": float(h[:, 2].mean() / target[0] - 1.0),
+                         "mu_rel_err": float(h[:, 3].mean() / target[1] - 1.0),
+                         "mu_ex_abs_err": float(h[:, 4].mean() - target[2]),
+                         "time_to_1pct_s": _time_to_target(r["rows"], target)})
+        else:
+            info.update({"steps": len(a), "time_to_1pct_s": None})
         out[tag] = info
     base = out["c128_si_dt0.005"]["time_to_1pct_s"]
-    lt = out["c64_learned_dt0.02"]["time_to_1pct_s"]
-    print(json.dumps({"metric": "time to Pi and mu within 1% of the complex128 semi-implicit dt=0.005 result",
-                      "unit": "s", "higher_is_better": False, "value": lt,
-                      "speedup_vs_c128": (base / lt) if (base and lt) else None,
-                      "target": {"Pi": target[0], "mu_poly_ex": target[1]}, "simulated_time": T,
-                      "config": {"workload": case.name + ": %d^3, L=%gb, N=50, divalent counterions, salt 0.05"
-                                 % (case.m[0], case.L[0])},
+    best = None
+    for tag, v in out.items():
+        if tag.startswith("c64_learned") and v["time_to_1pct_s"] and (best is None or v["time_to_1pct_s"] < best[1]):
+            best = (tag, v["time_to_1pct_s"])
+    print(json.dumps({"metric": "wall time for Pi and mu to settle within 1% of the complex128 semi-implicit "
+                                "dt=0.005 result", "unit": "s", "higher_is_better": False,
+                      "value": best[1] if best else None, "best_learned_run": best[0] if best else None,
+                      "c128_time_to_1pct_s": base,
+                      "speedup_vs_c128": (base / best[1]) if (base and best) else None,
+                      "target": {"Pi": target[0], "mu": target[1], "mu_ex": target[2],
+                                 "Pi_se": float(target_se[0]), "mu_se": float(target_se[1]),
+                                 "mu_ex_se": float(target_se[2])},
+                      "criterion": "running means over the second half of each trajectory, checked every 50 steps, "
+                                   "stay within 1% of the target from then on; mu = mu_ex + mu_self + mu_id of the "
+                                   "polymer (mu_ex alone averages near zero: its absolute error is reported)",
+                      "simulated_time": T,
+                      "config": {"workload": case.name + ": %d^3, L=%gb, N=%d, %s counterions, salt %g"
+                                 % (case.m[0], case.L[0], N,
+                                    "divalent" if case.counterions["valence"] == 2.0 else "monovalent", salt)},
                       "data": "synthetic", "runs": out}))
     return 0
 
@@ -722,8 +770,11 @@ def run_long(args, local):
     """`--long-run K` steps of the 128^3 workload (seeded noise, full stress),
     device time averages of the record (the reference's rule with Nss = 10,
     complexLangevin.cu:424-467, plus 10 blocks for the errors), device
-    checkpoints every 10 steps and the capped rollback (20): the run stops when
-    the cap is reached, as the reference's does."""
+    checkpoints every --checkpoint-every steps and the capped rollback
+    (--max-restarts): the run stops when the cap is reached, as the
+    reference's does.  With a checkpoint interval longer than the run, every
+    rollback restores the initial fields (the policy of the reference
+    harness's timing mode), so non-finite step counts compare directly."""
     import numpy as np
     import torch
     from ftspolysol_b200 import Engine, FP32, FP64, SCHEME_PC, SCHEME_SI
@@ -737,8 +788,8 @@ def run_long(args, local):
     d = derive(case)
     prec = FP32 if args.long_precision == "fp32" else FP64
     scheme = SCHEME_SI if args.long_scheme == "si" else SCHEME_PC
-    e = Engine(d, precision=prec, scheme=scheme, noise=True, seed=4321, device=local, restart_interval=10,
-               max_restarts=20)
+    e = Engine(d, precision=prec, scheme=scheme, noise=True, seed=4321, device=local,
+               restart_interval=args.checkpoint_every, max_restarts=args.max_restarts)
     om, ps = case.initial_fields()
     e.set_fields(om, ps)
     if args.adaptive > 0:
@@ -768,8 +819,8 @@ def run_long(args, local):
                       "config": {"workload": case.name + ": %d^3, L=%gb, N=50, divalent counterions, salt 0.05, "
                                  "full stress + Pi, seeded noise" % (case.m[0], case.L[0]),
                                  "precision": args.long_precision, "scheme": args.long_scheme, "dt": args.long_dt,
-                                 "adaptive_u_ref": args.adaptive or None, "Nss": case.Nss, "checkpoint_every": 10,
-                                 "max_restarts": 20},
+                                 "adaptive_u_ref": args.adaptive or None, "Nss": case.Nss,
+                                 "checkpoint_every": args.checkpoint_every, "max_restarts": args.max_restarts},
                       "averages": {n: {"mean": float(m), "se": float(s)} for n, m, s in zip(names, mean, se)}}))
     return 0
 

@@ -247,13 +247,18 @@ static __global__ void k_average(DevScal* d, double* acc, int R, long long skip,
     }
 }
 
+// Any block size that is a multiple of 32 (up to 1024): threads stride over
+// the rows, a shuffle tree per warp, then warp 0 combines the warps in order;
+// the summation order depends only on count and the block size.
+constexpr int COMBINE_THREADS = 256;
 template <bool MAX>
 __global__ void k_combine(const double* partial, int count, int K, double* out)
 {
+    __shared__ double ws[32];
     const int c = blockIdx.x;
     double s = 0.0;
     pdl_wait();
-    for (int b = threadIdx.x; b < count; b += 32) {
+    for (int b = threadIdx.x; b < count; b += blockDim.x) {
         const double y = partial[(size_t)b * K + c];
         s = MAX ? fmax(s, y) : s + y;
     }
@@ -262,7 +267,22 @@ __global__ void k_combine(const double* partial, int count, int K, double* out)
         const double y = __shfl_xor_sync(0xffffffffu, s, o);
         s = MAX ? fmax(s, y) : s + y;
     }
-    if (threadIdx.x == 0) out[c] = s;
+    const int nw = blockDim.x >> 5;
+    if (nw == 1) {
+        if (threadIdx.x == 0) out[c] = s;
+        return;
+    }
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < nw ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, s, o);
+            s = MAX ? fmax(s, y) : s + y;
+        }
+        if (threadIdx.x == 0) out[c] = s;
+    }
 }
 
 // ---- small complex helpers in double ----
@@ -1632,7 +1652,7 @@ struct Engine : EngineBase {
     {
         cudaEvent_t ev = bpe > 0.0 ? prof_begin() : nullptr;
         launch_pass(k_reduce<K, MAX, F>, dim3(RED_BLOCKS), RED_THREADS, 0, n, f, (double*)part.p);
-        launch_pass(k_combine<MAX>, dim3(K), 32, 0, (const double*)part.p, (int)RED_BLOCKS, (int)K, out);
+        launch_pass(k_combine<MAX>, dim3(K), COMBINE_THREADS, 0, (const double*)part.p, (int)RED_BLOCKS, (int)K, out);
         launches += 2;
         prof_end(ev, "field_reduce", bpe * (double)n);
     }
@@ -1944,7 +1964,7 @@ struct Engine : EngineBase {
             DevScal* d = ds;
             const int* eF = expo.p;
             const int last = N - 1;
-            k_combine<false><<<2, 32, 0, stream>>>(qpart, cnt, 2, reinterpret_cast<double*>(&d->Q[isp]));
+            k_combine<false><<<2, COMBINE_THREADS, 0, stream>>>(qpart, cnt, 2, reinterpret_cast<double*>(&d->Q[isp]));
             k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
                 const double2 Qs = dscale(d->Q[isp], invV);
                 d->factor[isp] = dscale(dinv(Qs), nv);
@@ -2721,7 +2741,7 @@ struct Engine : EngineBase {
     void finalize_record(bool with_stress)
     {
         if (with_stress) {
-            k_combine<false><<<12, 32, 0, stream>>>(spart.p, x_ctas(), 12, ds->sconn);
+            k_combine<false><<<12, COMBINE_THREADS, 0, stream>>>(spart.p, x_ctas(), 12, ds->sconn);
             ++launches;
         }
         const int S = (int)c.sp.size(), J = (int)c.ions.size(), nm = c.nm;
@@ -3373,7 +3393,7 @@ struct Engine : EngineBase {
             }
         }
         double* out = reinterpret_cast<double*>(&ds->Q[0]);
-        k_combine<false><<<2, 32, 0, stream>>>(part.p, seg_pass_ctas(), 2, out);
+        k_combine<false><<<2, COMBINE_THREADS, 0, stream>>>(part.p, seg_pass_ctas(), 2, out);
         ++launches;
         double q[2];
         FTSP_CUDA(cudaMemcpyAsync(q, out, sizeof(q), cudaMemcpyDeviceToHost, stream));
