@@ -678,6 +678,11 @@ struct Engine : EngineBase {
     bool chain_sym = true;       // use the pair kernels for mirror-symmetric species
     bool fused_strided = true;   // bond passes with register-resident middle stages (k_strided_fused)
     bool fused_plane = true;     // mid segment passes with register-resident end stages (k_plane_fused)
+    bool zreg_plane = true;      // forward mid passes of 128^2 complex64 planes: z pair in registers (k_plane_zreg)
+    // every ion smeared like the beads (and at most 3 ion species): the ion
+    // potentials are psi_s itself, and the ion charge is one combined field
+    // sum_j z_j (n_j/V)/Q_j exp(-i z_j psi_s), transformed once (see eval)
+    bool ion_common = false;
     int qF_holds_u = -1;         // species whose u = q / E the qF buffer holds (-1: q)
     // a single mirror-symmetric species runs its stress kernel on a second
     // stream, overlapped with the rest of the density evaluation
@@ -981,6 +986,8 @@ struct Engine : EngineBase {
         }
         if (gi.empty()) gi = sep(0.0);
         upload(gion, gi);
+        ion_common = c.elec && !c.ions.empty() && c.ions.size() <= 3;
+        for (auto& ion : c.ions) ion_common = ion_common && ion.smear == c.a;
         if (c.scheme == FTSP_SCHEME_SI) build_si_tables();
     }
 
@@ -1702,6 +1709,15 @@ struct Engine : EngineBase {
                 return;
             }
         }
+        if constexpr (S1 != 0 && S2 != 0 && F32 && N == 128 && NT == 1024 && op_loads<Op>::value <= 1) {
+            if (zreg_plane) {
+                auto k = k_plane_zreg<T, S1, S2, Op>;
+                set_smem(k, smem);
+                launch_pass(k, dim3(c.m1, nf), NT, smem, src, dst, (size_t)V_, (const V*)tw3.p, op);
+                ++launches;
+                return;
+            }
+        }
         if constexpr (S1 != 0 && S2 != 0 && plane_fused_ok<N, RMAX, NT, E>()) {
             if (fused_plane) {
                 auto k = k_plane_fused<T, N, RMAX, NT, E, S1, S2, Op>;
@@ -2264,6 +2280,7 @@ struct Engine : EngineBase {
             const T* gi = gion.p;
             const int sum_m = m1 + m2 + m3;
             const double invV = 1.0 / (double)Vn;
+            const int Jk = ion_common ? 0 : J;   // ion potentials of their own
             foreach(Vn, [=] __device__(size_t i) {
                 const int x = (int)(i / ((size_t)m2 * m3));
                 const int r = (int)(i - (size_t)x * m2 * m3);
@@ -2277,14 +2294,14 @@ struct Engine : EngineBase {
                 }
                 const double2 P = to_d(kAp[(size_t)nm * Vn + i]);
                 kBp[(size_t)M * Vn + i] = from_d<V>(elec ? dscale(P, gv) : make_double2(0.0, 0.0));
-                for (int j = 0; j < J; ++j) {
+                for (int j = 0; j < Jk; ++j) {
                     const T* t = gi + (size_t)j * sum_m;
                     const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
                     kBp[(size_t)(M + 1 + j) * Vn + i] = from_d<V>(elec ? dscale(P, gj) : make_double2(0.0, 0.0));
                 }
-            }, (double)(c.nm + 1 + c.M + 1 + J) * sizeof(V));
+            }, (double)(c.nm + 1 + c.M + 1 + Jk) * sizeof(V));
         }
-        fft3<+1>(kB.p, M + 1 + J);
+        fft3<+1>(kB.p, M + 1 + (ion_common ? 0 : J));
         // 3. class tables exp(-(W_type + i z psi_s)), ion Boltzmann factors, zeroed accumulators
         {
             ClsTab ct{};
@@ -2299,33 +2316,87 @@ struct Engine : EngineBase {
             const V* kBp = kB.p;
             V* Ep = E.p;
             V* dBp = dB.p;
-            foreach(Vn, [=] __device__(size_t i) {
-                const V ps_ = kBp[(size_t)M * Vn + i];
-                for (int k = 0; k < ncls; ++k) {
-                    V w = kBp[(size_t)ct.type[k] * Vn + i];
-                    const T zz = (T)ct.z[k];
-                    if (zz != T(0)) {   // W += psi_s * (0 + i z)  (add_scaled_complex_const)
-                        w.x += -(ps_.y * zz);
-                        w.y += ps_.x * zz;
+            if (ion_common) {
+                // the Boltzmann factors exp(-i z_j psi_s) are only summed here
+                // (Q_j); the combined ion charge is formed after the sweeps
+                reduce<6>(Vn, [=] __device__(size_t i, double* acc) {
+                    const V ps_ = kBp[(size_t)M * Vn + i];
+                    for (int k = 0; k < ncls; ++k) {
+                        V w = kBp[(size_t)ct.type[k] * Vn + i];
+                        const T zz = (T)ct.z[k];
+                        if (zz != T(0)) {
+                            w.x += -(ps_.y * zz);
+                            w.y += ps_.x * zz;
+                        }
+                        Ep[(size_t)k * Vn + i] = cexpT(-w.x, -w.y);
                     }
-                    Ep[(size_t)k * Vn + i] = cexpT(-w.x, -w.y);
-                }
-                for (int al = 0; al <= M; ++al) dBp[(size_t)al * Vn + i] = mkc<V>(T(0), T(0));
-                for (int j = 0; j < J; ++j) {
-                    const V pj = kBp[(size_t)(M + 1 + j) * Vn + i];
-                    const T zz = (T)zi.z[j];
-                    dBp[(size_t)(M + 1 + j) * Vn + i] = cexpT(zz * pj.y, -zz * pj.x);
-                }
-            }, (double)(2 * (c.M + 1 + J) + (int)c.cls.size()) * sizeof(V));
+                    for (int al = 0; al <= M; ++al) dBp[(size_t)al * Vn + i] = mkc<V>(T(0), T(0));
+                    for (int j = 0; j < J; ++j) {
+                        const T zz = (T)zi.z[j];
+                        const V b = cexpT(zz * ps_.y, -zz * ps_.x);
+                        acc[2 * j] += (double)b.x;
+                        acc[2 * j + 1] += (double)b.y;
+                    }
+                }, reinterpret_cast<double*>(&ds->Qion[0]), (double)(2 + 2 * c.M + (int)c.cls.size()) * sizeof(V));
+                DevScal* d = ds;
+                IonTab ic{};
+                for (int j = 0; j < J; ++j) ic.nd[j] = c.ions[j].count / c.volume;
+                const double invV = 1.0 / (double)Vn;
+                k_foreach<<<1, 32, 0, stream>>>((size_t)J, [=] __device__(size_t j) {
+                    const double2 Q = dscale(d->Qion[j], invV);
+                    d->Qion[j] = Q;
+                    d->ion_factor[j] = dscale(dinv(Q), ic.nd[j]);
+                });
+                ++launches;
+            } else {
+                foreach(Vn, [=] __device__(size_t i) {
+                    const V ps_ = kBp[(size_t)M * Vn + i];
+                    for (int k = 0; k < ncls; ++k) {
+                        V w = kBp[(size_t)ct.type[k] * Vn + i];
+                        const T zz = (T)ct.z[k];
+                        if (zz != T(0)) {   // W += psi_s * (0 + i z)  (add_scaled_complex_const)
+                            w.x += -(ps_.y * zz);
+                            w.y += ps_.x * zz;
+                        }
+                        Ep[(size_t)k * Vn + i] = cexpT(-w.x, -w.y);
+                    }
+                    for (int al = 0; al <= M; ++al) dBp[(size_t)al * Vn + i] = mkc<V>(T(0), T(0));
+                    for (int j = 0; j < J; ++j) {
+                        const V pj = kBp[(size_t)(M + 1 + j) * Vn + i];
+                        const T zz = (T)zi.z[j];
+                        dBp[(size_t)(M + 1 + j) * Vn + i] = cexpT(zz * pj.y, -zz * pj.x);
+                    }
+                }, (double)(2 * (c.M + 1 + J) + (int)c.cls.size()) * sizeof(V));
+            }
         }
         if (stress) FTSP_CUDA(cudaMemsetAsync(spart.p, 0, sizeof(double) * 12 * (size_t)x_ctas(), stream));
         // 4. chain propagators of every species
         for (int isp = 0; isp < (int)c.sp.size(); ++isp) solve_species(isp, stress);
         charge_fold();
-        // 5. DFT of the raw densities and the ion Boltzmann factors
-        fft3<-1>(dB.p, M + 1 + J);
+        if (ion_common) {
+            // the combined ion charge sum_j z_j (n_j/V)/Q_j exp(-i z_j psi_s)
+            // (ion_density_from_psi, common.h:1117-1130, summed over the
+            // species before the smoothing, which is common to all of them)
+            const V* ps = kB.p + (size_t)M * Vn;
+            V* cion = dB.p + (size_t)(M + 1) * Vn;
+            IonTab zi{};
+            for (int j = 0; j < J; ++j) zi.z[j] = c.ions[j].z;
+            const DevScal* d = ds;
+            foreach(Vn, [=] __device__(size_t i) {
+                const V p = ps[i];
+                double2 acc = make_double2(0.0, 0.0);
+                for (int j = 0; j < J; ++j) {
+                    const T zz = (T)zi.z[j];
+                    acc = dadd(acc, dscale(dmul(to_d(cexpT(zz * p.y, -zz * p.x)), d->ion_factor[j]), zi.z[j]));
+                }
+                cion[i] = from_d<V>(acc);
+            }, 2.0 * sizeof(V));
+        }
+        const int Jd = ion_common ? 1 : J;   // ion fields of the density transform
+        // 5. DFT of the raw densities and the ion Boltzmann factors (or the combined ion charge)
+        fft3<-1>(dB.p, M + 1 + Jd);
         // 6. ion partition functions from the DC bins
-        if (J > 0) {
+        if (J > 0 && !ion_common) {
             DevScal* d = ds;
             const V* dBp = dB.p;
             IonTab ic{};
@@ -2354,6 +2425,7 @@ struct Engine : EngineBase {
             IonTab zi{};
             for (int j = 0; j < J; ++j) zi.z[j] = elec ? c.ions[j].z : 0.0;
             const DevScal* d = ds;
+            const bool common = ion_common;
             foreach(Vn, [=] __device__(size_t i) {
                 const int x = (int)(i / ((size_t)m2 * m3));
                 const int r = (int)(i - (size_t)x * m2 * m3);
@@ -2361,16 +2433,20 @@ struct Engine : EngineBase {
                 const double gv = (double)(gm[x] * gm[m1 + y] * gm[m1 + m2 + z]) * invV;
                 for (int al = 0; al <= M; ++al) kCp[(size_t)al * Vn + i] = from_d<V>(dscale(to_d(dBp[(size_t)al * Vn + i]), gv));
                 double2 ci = make_double2(0.0, 0.0);
-                for (int j = 0; j < J; ++j) {
-                    const T* t = gi + (size_t)j * sum_m;
-                    const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
-                    const double2 f = d->ion_factor[j];
-                    ci = dadd(ci, dscale(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + i]), f), gj * zi.z[j]));
+                if (common) {   // the combined ion charge, smoothed like the beads
+                    ci = dscale(to_d(dBp[(size_t)(M + 1) * Vn + i]), gv);
+                } else {
+                    for (int j = 0; j < J; ++j) {
+                        const T* t = gi + (size_t)j * sum_m;
+                        const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]) * invV;
+                        const double2 f = d->ion_factor[j];
+                        ci = dadd(ci, dscale(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + i]), f), gj * zi.z[j]));
+                    }
                 }
                 kCp[(size_t)(M + 1) * Vn + i] = from_d<V>(ci);
                 const double k2 = kxp[x] * kxp[x] + kyp[y] * kyp[y] + kzp[z] * kzp[z];
                 kCp[(size_t)(M + 2) * Vn + i] = from_d<V>(dscale(to_d(kAp[(size_t)nm * Vn + i]), k2 * invV * dpsi_scale));
-            }, (double)(2 * c.M + 5 + J) * sizeof(V));
+            }, (double)(2 * c.M + 5 + Jd) * sizeof(V));
         }
         fft3<+1>(kC.p, M + 3);
         // 8. real-space epilogue: rho_p, rho_c, ion densities, raw psi drift (+ its sum)
@@ -2387,6 +2463,7 @@ struct Engine : EngineBase {
                 iz.z[j] = c.ions[j].z;
                 iz.nd[j] = c.ions[j].count / c.volume;
             }
+            const bool common = ion_common;
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
                 V sum = mkc<V>(T(0), T(0));
                 for (int al = 0; al < M; ++al) sum = cadd(sum, kCp[(size_t)al * Vn + i]);
@@ -2397,7 +2474,7 @@ struct Engine : EngineBase {
                 rc[i] = rcv;
                 for (int j = 0; j < J; ++j) {
                     if (elec) {
-                        const V pj = kBp[(size_t)(M + 1 + j) * Vn + i];
+                        const V pj = kBp[(size_t)(common ? M : M + 1 + j) * Vn + i];
                         const T zz = (T)iz.z[j];
                         const V b = cexpT(zz * pj.y, -zz * pj.x);
                         ir[(size_t)j * Vn + i] = cmul(b, from_d<V>(d->ion_factor[j]));
@@ -2415,7 +2492,7 @@ struct Engine : EngineBase {
                 dp[i] = dv;
                 acc[0] += (double)dv.x;
                 acc[1] += (double)dv.y;
-            }, reinterpret_cast<double*>(&ds->mean_dpsi), (double)(c.M + 6 + 2 * J) * sizeof(V));
+            }, reinterpret_cast<double*>(&ds->mean_dpsi), (double)(c.M + 6 + J + (common ? 0 : J)) * sizeof(V));
         }
         // when electrostatics are off the charge fields stay zero
         if (!elec) {
@@ -2694,6 +2771,7 @@ struct Engine : EngineBase {
         const double* kzp = kz.p;
         const int sum_m = m1 + m2 + m3;
         const DevScal* d = ds;
+        const bool common = ion_common;
         reduce<26>(Vn, [=] __device__(size_t i, double* acc) {
             const int x = (int)(i / ((size_t)m2 * m3));
             const int r = (int)(i - (size_t)x * m2 * m3);
@@ -2716,13 +2794,21 @@ struct Engine : EngineBase {
                 const double2 Pm = to_d(kAp[(size_t)nm * Vn + ineg]);
                 const double2 rc = dmul(to_d(dBp[(size_t)M * Vn + ineg]), dscale(Pk, Gk));
                 Bc = make_double2(-rc.y, rc.x);   // i * R_c(-k) Gamma Psi(k)
-                for (int j = 0; j < J; ++j) {
-                    const T* t = gi + (size_t)j * sum_m;
-                    const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]);
-                    const double2 p = dmul(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + ineg]), d->ion_factor[j]), dscale(Pk, gj * oc.z[j]));
+                if (common) {
+                    // combined ion charge (z_j (n_j/V)/Q_j already in it), common smearing
+                    const double2 p = dmul(to_d(dBp[(size_t)(M + 1) * Vn + ineg]), dscale(Pk, Gk));
                     const double2 ip = make_double2(-p.y, p.x);
-                    Ij = dadd(Ij, dscale(ip, -oc.a2ion[j]));
-                    I0 = dadd(I0, dscale(ip, 1.0 / 6.0));
+                    Ij = dscale(ip, -oc.a2ion[0]);
+                    I0 = dscale(ip, 1.0 / 6.0);
+                } else {
+                    for (int j = 0; j < J; ++j) {
+                        const T* t = gi + (size_t)j * sum_m;
+                        const double gj = (double)(t[x] * t[m1 + y] * t[m1 + m2 + z]);
+                        const double2 p = dmul(dmul(to_d(dBp[(size_t)(M + 1 + j) * Vn + ineg]), d->ion_factor[j]), dscale(Pk, gj * oc.z[j]));
+                        const double2 ip = make_double2(-p.y, p.x);
+                        Ij = dadd(Ij, dscale(ip, -oc.a2ion[j]));
+                        I0 = dadd(I0, dscale(ip, 1.0 / 6.0));
+                    }
                 }
                 X = dmul(Pk, Pm);
             }
@@ -2735,7 +2821,7 @@ struct Engine : EngineBase {
             }
             acc[12] += 0.5 * A.x + Bc.x / 6.0 + I0.x;
             acc[13] += 0.5 * A.y + Bc.y / 6.0 + I0.y;
-        }, ds->kobs, (double)(c.nm + c.M + 2 + (int)c.ions.size()) * sizeof(V));
+        }, ds->kobs, (double)(c.nm + c.M + 2 + (ion_common ? 1 : (int)c.ions.size())) * sizeof(V));
     }
 
     void finalize_record(bool with_stress)

@@ -19,6 +19,8 @@
 
 #include "fft_core.cuh"
 
+#include <type_traits>
+
 namespace ftsp {
 
 // Programmatic dependent launch: a pass launched with the programmatic
@@ -1143,6 +1145,191 @@ __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, 
         __syncthreads();
         ct_fft<V, S2, N, RMAX, BR, 1, P, NT, E>(tile, stw);
         for (int e = threadIdx.x; e < NE; e += NT) dst[base + e] = tile[(e / N) * P + e % N];
+    }
+    op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
+}
+
+
+// ---------------------------------------------------------------------------
+// Plane pass of a mid segment for 128^2 complex64 planes, with the z-transform
+// pair around the pointwise step held in registers.
+//
+// The inverse transform runs y then z, the forward one z then y; both are
+// radix 16 x 8 per axis (Stockham, autosorting).  The inverse z-transform ends
+// with its radix-8 stage and the forward one starts with radix 8 (reversed
+// radix order), so one thread holds the outputs i + 16t (t < 8) of butterfly i
+// of a z-row, applies the pointwise op to them and runs the first forward
+// butterfly on the same registers: no shared-memory round trip for the
+// pointwise step, and none between the two z-transforms.  For those two
+// stages the 16 butterflies of a row go to 16 consecutive threads, so a
+// half-warp touches 16 consecutive z (128 bytes) of one row in global memory
+// (the op's loads and stores are coalesced).  The forward stage writes
+// positions 8i + t, a stride of 8 complex values; the tile's z index is
+// swizzled, z ^ ((z >> 4) & 7), which keeps every half-warp access of every
+// stage on 16 distinct 8-byte bank slots (rows are padded to 129 values, so
+// accesses along y are spread by the row as well).
+//
+// Shared-memory round trips: 6 (y: 2, z: 2, z: 2 less the fused pair, y: 2
+// less the register-resident first and last stages); barriers: 11.  Same
+// grid, Op interface (forward ops: one load per point) and results, up to
+// the rounding of the operation order, as k_plane_fused.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int plane_swz(int z) { return z ^ ((z >> 4) & 7); }
+
+// Global loads per point of a pointwise op (Op::LOADS where declared, else 4).
+template <class Op, class = void>
+struct op_loads {
+    static constexpr int value = 4;
+};
+template <class Op>
+struct op_loads<Op, std::void_t<decltype(Op::LOADS)>> {
+    static constexpr int value = Op::LOADS;
+};
+
+// Twiddles of butterfly k of a stage with twiddle step 1 (N / (R * SPAN) = 1),
+// then the radix-R DFT.
+template <int S, int R, typename V>
+__device__ __forceinline__ void bfly_k(V (&u)[R], int k, const V* __restrict__ tw)
+{
+    if (k) {
+#pragma unroll
+        for (int t = 1; t < R; ++t) u[t] = cmul(u[t], twiddle<S>(tw, t * k));
+    }
+    dftR<S, R>(u);
+}
+
+template <typename T, int S1, int S2, class Op>
+__global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx<T>* dst, size_t fstride,
+                                                        const cplx<T>* __restrict__ twn, Op op)
+{
+    using V = cplx<T>;
+    constexpr int N = 128, P = N + 1, NE = N * N;
+    static_assert(S1 != 0 && S2 != 0, "both transforms");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* stw = tile + N * P;
+    const int tid = threadIdx.x;
+    const int x = blockIdx.x;
+    const int f = blockIdx.y;
+    const size_t base = (size_t)f * fstride + (size_t)x * NE;
+    for (int j = tid; j < N; j += 1024) stw[j] = twn[j];
+    if (tid == 0) op.prefetch(base, (unsigned)NE);   // L2 prefetch: cannot observe a stale value
+    pdl_wait();
+    const int zc = tid & 127;   // column of the y-stages
+    const int hi = tid >> 7;    // 0..7
+    // inverse y, stage 0 (radix 16, span 1): the coalesced load of column zc,
+    // rows hi + 8t, is the input set of butterfly hi
+    {
+        V u[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) u[t] = src[base + tid + t * 1024];
+        __syncthreads();   // twiddles
+        dftR<S1, 16>(u);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) tile[(16 * hi + t) * P + plane_swz(zc)] = u[t];
+        __syncthreads();
+    }
+    // inverse y, stage 1 (radix 8, span 16): butterflies hi and hi + 8 of column zc
+    {
+        V u[2][8];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) u[q][t] = tile[(hi + 8 * q + 16 * t) * P + plane_swz(zc)];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            bfly_k<S1, 8>(u[q], hi + 8 * q, stw);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) tile[(hi + 8 * q + 16 * t) * P + plane_swz(zc)] = u[q][t];
+        }
+        __syncthreads();
+    }
+    // inverse z, stage 0 (radix 16, span 1): row zc (line-fastest), butterfly hi
+    {
+        const int y = zc;
+        V u[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(hi + 8 * t)];
+        __syncthreads();
+        dftR<S1, 16>(u);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(16 * hi + t)] = u[t];
+        __syncthreads();
+    }
+    op.begin();
+    // inverse z, stage 1 (radix 8, span 16) -> op -> forward z, stage 0
+    // (radix 8, span 1): butterfly i = tid & 15 of rows yq = tid/16 + 64q
+    {
+        const int i = tid & 15;
+        V u[2][8];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int y = (tid >> 4) + 64 * q;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) u[q][t] = tile[y * P + plane_swz(i + 16 * t)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int y = (tid >> 4) + 64 * q;
+            bfly_k<S1, 8>(u[q], i, stw);
+            typename Op::Pre pre[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) pre[t] = op.load(f, base + (size_t)y * N + i + 16 * t);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int z = i + 16 * t;
+                u[q][t] = op.apply(f, x, y, z, base + (size_t)y * N + z, u[q][t], pre[t]);
+            }
+        }
+        pdl_trigger();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int y = (tid >> 4) + 64 * q;
+            dftR<S2, 8>(u[q]);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) tile[y * P + plane_swz(8 * i + t)] = u[q][t];
+        }
+        __syncthreads();
+    }
+    // forward z, stage 1 (radix 16, span 8): row zc, butterfly hi
+    {
+        const int y = zc;
+        V u[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(hi + 8 * t)];
+        __syncthreads();
+        bfly_k<S2, 16>(u, hi, stw);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(hi + 8 * t)] = u[t];
+        __syncthreads();
+    }
+    // forward y, stage 0 (radix 16, span 1): column zc, butterfly hi
+    {
+        V u[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) u[t] = tile[(hi + 8 * t) * P + plane_swz(zc)];
+        __syncthreads();
+        dftR<S2, 16>(u);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) tile[(16 * hi + t) * P + plane_swz(zc)] = u[t];
+        __syncthreads();
+    }
+    // forward y, stage 1 (radix 8, span 16): butterflies hi and hi + 8 of
+    // column zc, stored straight to global memory (consecutive z per warp)
+    {
+        V u[2][8];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) u[q][t] = tile[(hi + 8 * q + 16 * t) * P + plane_swz(zc)];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            bfly_k<S2, 8>(u[q], hi + 8 * q, stw);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) dst[base + (size_t)(hi + 8 * q + 16 * t) * N + zc] = u[q][t];
+        }
     }
     op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
 }
