@@ -161,6 +161,13 @@ int ftsp_set_fields(ftsp_handle* h, const double* omega, const double* psi)
     return FTSP_OK;
 }
 
+int ftsp_set_fields_async(ftsp_handle* h, const double* omega, const double* psi)
+{
+    if (!psi) return FTSP_ERROR;
+    FTSP_GUARD(h, h->eng->set_fields_async(omega, psi));
+    return FTSP_OK;
+}
+
 int ftsp_get_field(ftsp_handle* h, const char* name, double* out, long long* count)
 {
     long long n = -1;
@@ -500,6 +507,7 @@ int ftsp_batch_create(ftsp_handle* const* handles, int n, int steps_per_graph, f
             b->ev.push_back(e);
         }
         // finish whatever the handles queued on their own streams
+        for (auto* h : b->hs) h->eng->install_pending_fields();   // before the capture
         for (auto* h : b->hs) batch_check(cudaStreamSynchronize(h->eng->stream), "cudaStreamSynchronize");
         for (int i = 0; i < n; ++i) {
             b->saved.push_back(b->hs[i]->eng->stream);

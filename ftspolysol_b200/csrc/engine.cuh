@@ -581,6 +581,8 @@ struct EngineBase {
     }
     virtual ~EngineBase() {}
     virtual void set_fields(const double* omega, const double* psi) = 0;
+    virtual void set_fields_async(const double* omega, const double* psi) = 0;
+    virtual void install_pending_fields() = 0;
     virtual long long get_field(const std::string& name, double* out) = 0;
     virtual void compute_densities(int which, double* Q) = 0;
     virtual void measure(int which, double* rec) = 0;
@@ -714,6 +716,13 @@ struct Engine : EngineBase {
         if (aux) cudaStreamDestroy(aux);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (cstream) {
+            cudaStreamSynchronize(cstream);
+            cudaStreamDestroy(cstream);
+        }
+        if (ev_staged) cudaEventDestroy(ev_staged);
+        if (ev_installed) cudaEventDestroy(ev_installed);
+        astage.release();
         Buf<V>* vb[] = {&tw1, &tw2, &tw3, &omega, &psi, &omega_bar, &psi_bar, &drift, &drift_bar, &dpsi, &dpsi_bar,
                         &kA, &kB, &dB, &kC, &rho_p, &rho_c, &ion_rho, &E, &qF, &Fst, &G, &H};
         for (auto* b : vb) b->release();
@@ -2938,6 +2947,7 @@ struct Engine : EngineBase {
 
     void set_fields(const double* om, const double* ps) override
     {
+        drop_pending_fields();
         const size_t Vn = V_;
         const int nm = c.nm;
         if (sizeof(T) == 8) {
@@ -2947,14 +2957,85 @@ struct Engine : EngineBase {
             if (!stage.p) stage.alloc((size_t)(nm + 1) * Vn);
             if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(stage.p, om, sizeof(double2) * nm * Vn, cudaMemcpyHostToDevice, stream));
             FTSP_CUDA(cudaMemcpyAsync(stage.p + (size_t)nm * Vn, ps, sizeof(double2) * Vn, cudaMemcpyHostToDevice, stream));
-            const double2* s = stage.p;
-            V* o = omega.p;
-            V* p = psi.p;
-            foreach(Vn, [=] __device__(size_t i) {
-                for (int a = 0; a < nm; ++a) o[(size_t)a * Vn + i] = from_d<V>(s[(size_t)a * Vn + i]);
-                p[i] = from_d<V>(s[(size_t)nm * Vn + i]);
-            });
+            convert_staged(stage.p);
         }
+        new_run();
+        FTSP_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // FP64 fields in device memory (modes, then psi) into the working precision
+    void convert_staged(const double2* s)
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        V* o = omega.p;
+        V* p = psi.p;
+        foreach(Vn, [=] __device__(size_t i) {
+            for (int a = 0; a < nm; ++a) o[(size_t)a * Vn + i] = from_d<V>(s[(size_t)a * Vn + i]);
+            p[i] = from_d<V>(s[(size_t)nm * Vn + i]);
+        });
+    }
+
+    // ---- fields uploaded while the previous step runs ----
+    // set_fields_async copies the host fields into a device staging buffer on
+    // a copy stream and returns; the next call that uses the fields installs
+    // them on the handle's stream (after the copy, by an event): conversion,
+    // psi mean removal, a new run.  A second upload first waits until the
+    // staging buffer has been installed.
+    Buf<double2> astage;
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_staged = nullptr, ev_installed = nullptr;
+    bool fields_pending = false, astage_used = false;
+
+    void set_fields_async(const double* om, const double* ps) override
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        if (!cstream) {
+            FTSP_CUDA(cudaStreamCreateWithFlags(&cstream, cudaStreamNonBlocking));
+            FTSP_CUDA(cudaEventCreateWithFlags(&ev_staged, cudaEventDisableTiming));
+            FTSP_CUDA(cudaEventCreateWithFlags(&ev_installed, cudaEventDisableTiming));
+            astage.alloc((size_t)(nm + 1) * Vn);
+        }
+        if (fields_pending) install_pending_fields();   // one staging buffer
+        if (astage_used) FTSP_CUDA(cudaStreamWaitEvent(cstream, ev_installed, 0));
+        if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(astage.p, om, sizeof(double2) * nm * Vn, cudaMemcpyHostToDevice, cstream));
+        FTSP_CUDA(cudaMemcpyAsync(astage.p + (size_t)nm * Vn, ps, sizeof(double2) * Vn, cudaMemcpyHostToDevice, cstream));
+        FTSP_CUDA(cudaEventRecord(ev_staged, cstream));
+        fields_pending = true;
+    }
+
+    void install_pending_fields() override
+    {
+        if (!fields_pending) return;
+        fields_pending = false;
+        const size_t Vn = V_;
+        const int nm = c.nm;
+        FTSP_CUDA(cudaStreamWaitEvent(stream, ev_staged, 0));
+        if (sizeof(T) == 8) {
+            if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(omega.p, astage.p, sizeof(double2) * nm * Vn, cudaMemcpyDeviceToDevice, stream));
+            FTSP_CUDA(cudaMemcpyAsync(psi.p, astage.p + (size_t)nm * Vn, sizeof(double2) * Vn, cudaMemcpyDeviceToDevice, stream));
+        } else {
+            convert_staged(astage.p);
+        }
+        new_run();
+        FTSP_CUDA(cudaEventRecord(ev_installed, stream));
+        astage_used = true;
+    }
+
+    // a synchronous set_fields supersedes an upload not yet installed
+    void drop_pending_fields()
+    {
+        if (!fields_pending) return;
+        FTSP_CUDA(cudaEventSynchronize(ev_staged));
+        fields_pending = false;
+    }
+
+    // psi zero mode, run state and first checkpoint of freshly loaded fields
+    void new_run()
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm;
         if (c.elec) {
             const V* p = psi.p;
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
@@ -2973,11 +3054,11 @@ struct Engine : EngineBase {
             if (nm > 0) FTSP_CUDA(cudaMemcpyAsync(ck.p, omega.p, sizeof(V) * nm * Vn, cudaMemcpyDeviceToDevice, stream));
             FTSP_CUDA(cudaMemcpyAsync(ck.p + (size_t)nm * Vn, psi.p, sizeof(V) * Vn, cudaMemcpyDeviceToDevice, stream));
         }
-        FTSP_CUDA(cudaStreamSynchronize(stream));
     }
 
     long long get_field(const std::string& name, double* out) override
     {
+        install_pending_fields();
         const size_t Vn = V_;
         const int nm = c.nm, M = c.M, J = (int)c.ions.size();
         const V* p = nullptr;
@@ -3097,6 +3178,7 @@ struct Engine : EngineBase {
 
     void compute_densities(int which, double* Q) override
     {
+        install_pending_fields();
         eval(which, false);
         pull_scalars();
         if (Q)
@@ -3122,6 +3204,7 @@ struct Engine : EngineBase {
 
     void measure(int which, double* rec) override
     {
+        install_pending_fields();
         const bool st = c.stress_on();
         eval(which, st);
         field_squares(which);
@@ -3383,6 +3466,7 @@ struct Engine : EngineBase {
 
     int step(double* Qbar, double* rec, double* dmax, bool sync) override
     {
+        install_pending_fields();
         launches = 0;
         if (step_graph_usable()) {
             if (!sg_exec) capture_step();

@@ -103,6 +103,7 @@ def lib():
         L.ftsp_last_error.argtypes = [vp]
         L.ftsp_set_stream.argtypes = [vp, vp]
         L.ftsp_set_fields.argtypes = [vp, vp, vp]
+        L.ftsp_set_fields_async.argtypes = [vp, vp, vp]
         L.ftsp_get_field.argtypes = [vp, C.c_char_p, vp, C.POINTER(C.c_longlong)]
         L.ftsp_compute_densities.argtypes = [vp, C.c_int, vp]
         L.ftsp_record_length.argtypes = [vp]
@@ -157,6 +158,7 @@ def lib():
 
 # exported symbols of include/ftsp.h
 ABI_SYMBOLS = ("ftsp_create", "ftsp_destroy", "ftsp_last_error", "ftsp_set_stream", "ftsp_set_fields",
+               "ftsp_set_fields_async",
                "ftsp_get_field", "ftsp_compute_densities", "ftsp_record_length", "ftsp_measure",
                "ftsp_set_noise", "ftsp_set_seed", "ftsp_step", "ftsp_step_async", "ftsp_read_status",
                "ftsp_state_views", "ftsp_last_launch_count", "ftsp_profile_enable", "ftsp_profile_read",
@@ -336,6 +338,12 @@ class Engine:
     def set_fields_ptr(self, omega_ptr: int, psi_ptr: int):
         """set_fields from raw host pointers (e.g. pinned buffers)."""
         self._check(lib().ftsp_set_fields(self.h, C.c_void_p(omega_ptr), C.c_void_p(psi_ptr)), "set_fields")
+
+    def set_fields_async_ptr(self, omega_ptr: int, psi_ptr: int):
+        """Upload of new fields from (pinned) host memory that overlaps the
+        step in flight; installed by the next call that uses the fields.
+        The host buffers must stay unchanged until results have been read."""
+        self._check(lib().ftsp_set_fields_async(self.h, C.c_void_p(omega_ptr), C.c_void_p(psi_ptr)), "set_fields_async")
 
     def propagate_chain(self, w_ptr: int, N: int, bond_length: float, q_end_ptr: int) -> complex:
         """Chain propagation in an external field (device pointers, complex128)."""

@@ -105,6 +105,19 @@ int ftsp_set_stream(ftsp_handle* h, void* cuda_stream);
  * float64) and removes the psi zero mode (complexLangevin.cu:182-183). */
 int ftsp_set_fields(ftsp_handle* h, const double* omega, const double* psi);
 
+/* ftsp_set_fields without waiting (no reference counterpart: the reference
+ * copies its fields in once, complexLangevin.cu:166-191).  The fields are
+ * copied from host memory into a device staging buffer on a separate copy
+ * stream, so that an upload overlaps the step still running; the next call
+ * that uses the fields (ftsp_step, ftsp_step_async, ftsp_compute_densities,
+ * ftsp_measure, ftsp_get_field, ftsp_batch_create) installs them on the
+ * handle's stream first, with the same effect as ftsp_set_fields.  With
+ * pinned host memory the call returns at once; the host buffers must stay
+ * unchanged until a later call has returned results to the host
+ * (ftsp_step, ftsp_read_status, ftsp_get_field).  A synchronous
+ * ftsp_set_fields supersedes an upload that is not yet installed. */
+int ftsp_set_fields_async(ftsp_handle* h, const double* omega, const double* psi);
+
 /* Copies a named field to host memory as interleaved complex float64.
  * Names follow deviceState (deviceState.h:6-48): omega psi omega_bar psi_bar
  * drift drift_bar dpsi dpsi_bar rho_type rho_p rho_c rho_c_poly rho_c_ion
