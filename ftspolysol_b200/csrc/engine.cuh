@@ -434,18 +434,154 @@ struct OpPrecond {
     const DevScal* d;
     SigTab st;               // dt lambda_f per field
     T invV;
+    int dc0 = -1;            // field whose k = 0 value is set to zero (psi: its mean removal), -1: none
     static constexpr int FUSED_MIN_BLOCKS = 8;
     struct Pre {};
     __device__ __forceinline__ void begin() {}
     __device__ __forceinline__ Pre load(int, size_t) const { return Pre{}; }
-    __device__ __forceinline__ cplx<T> apply(int f, int, int, int, size_t g, cplx<T> v, const Pre&) const
+    __device__ __forceinline__ cplx<T> apply(int f, int x, int y, int z, size_t g, cplx<T> v, const Pre&) const
     {
         const T G = (GL && d->lr_use) ? GL[g] : GA[g];
         const cplx<T> k = cscale(v, (T)(1.0 / (1.0 + (st.s[f] * d->dt_scale) * (double)G)));
         if (dw) dw[g] = k;
+        if (f == dc0 && (x | y | z) == 0) return mkc<cplx<T>>(T(0), T(0));
         return cscale(k, invV);
     }
     __device__ __forceinline__ void end(double*, size_t) {}
+};
+
+// The increments of the semi-implicit update, computed as the field loads of
+// its first transform pass (the load of field f at point g; f < nm the
+// interaction modes, f = nm psi):
+//   predictor: dt_scale c_f u_f + eta_f, psi: its noise and drift with their
+//              means removed first (written back: the corrector reads them);
+//   corrector: dt_scale c_f (u_f + u_bar_f) + eta_f, psi: the predictor drift
+//              plus the mean-removed u_bar (written back); and the largest
+//              |u + u_bar|^2 of the CTA's points, per field, into dpart
+//              (the drift maxima, complexLangevin.cu:474-498).
+// c_f = -dt lambda_f (predictor), -dt lambda_f / 2 (corrector).
+template <typename T, bool CORR>
+struct OpIncrement {
+    using V = cplx<T>;
+    const V* u0;             // drift at (omega, psi)
+    const V* u1;             // drift at (omega_bar, psi_bar) (corrector)
+    T* e;                    // noise, nm + 1 real fields
+    V* dp;                   // psi drift at (omega, psi)
+    V* db;                   // psi drift at (omega_bar, psi_bar) (corrector)
+    const DevScal* d;
+    ModeTab co;              // c_f of the modes
+    double sp;               // c_f of psi
+    double invV;
+    size_t Vn;
+    int nm;
+    bool elec;
+    double* dpart;           // corrector: per-CTA drift maxima [cta][nm + 1]
+    mutable double dmax;
+    struct Pre {
+        V v;
+    };
+    __device__ __forceinline__ void begin() { dmax = 0.0; }
+    __device__ __forceinline__ Pre load(int f, size_t g) const
+    {
+        const size_t i = g - (size_t)f * Vn;
+        if (f < nm) {
+            const size_t j = (size_t)f * Vn + i;
+            V s = u0[j];
+            if (CORR) {
+                s = cadd(s, u1[j]);
+                double m = (double)s.x * s.x + (double)s.y * s.y;
+                if (!isfinite(m)) m = INFINITY;
+                dmax = fmax(dmax, m);
+            }
+            V v = cscale(s, (T)(co.s[f] * d->dt_scale));
+            v.x += e[j];
+            return Pre{v};
+        }
+        if (!elec) return Pre{mkc<V>(T(0), T(0))};
+        const size_t j = (size_t)nm * Vn + i;
+        T ep = e[j];
+        if (!CORR) {
+            ep = (T)((double)ep + (-(d->mean_eta * invV)));
+            e[j] = ep;
+        }
+        // mean_dpsi: the sum of the psi drift of the last density evaluation
+        // (at omega, psi for the predictor; at the predictor's fields for the corrector)
+        V s;
+        if (!CORR) {
+            s = cadd(dp[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+            dp[i] = s;
+        } else {
+            const V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+            db[i] = dbv;
+            s = cadd(dp[i], dbv);
+            double m = (double)s.x * s.x + (double)s.y * s.y;
+            if (!isfinite(m)) m = INFINITY;
+            dmax = fmax(dmax, m);
+        }
+        V v = cscale(s, (T)(sp * d->dt_scale));
+        v.x += ep;
+        return Pre{v};
+    }
+    __device__ __forceinline__ V apply(int, int, int, int, size_t, V, const Pre& p) const { return p.v; }
+    __device__ __forceinline__ void end(double* scratch, size_t cta)
+    {
+        if (!CORR) return;
+        __syncthreads();
+        double m = dmax;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 0.0;
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) r = fmax(r, scratch[w]);
+            dpart[cta] = r;
+        }
+    }
+};
+
+// The last pass of the semi-implicit update: field f = base f + increment
+// (predictor: omega_bar, psi_bar from omega, psi; corrector: omega, psi in
+// place), and the count of non-finite cells per CTA into npart.
+template <typename T>
+struct OpUpdate {
+    using V = cplx<T>;
+    const V* w0;             // modes before the update
+    const V* p0;             // psi before the update
+    V* w1;                   // modes after
+    V* p1;                   // psi after
+    size_t Vn;
+    int nm;
+    bool elec;
+    double* npart;           // per-CTA non-finite counts (null: not counted)
+    double bad;
+    struct Pre {
+        V b;
+    };
+    __device__ __forceinline__ void begin() { bad = 0.0; }
+    __device__ __forceinline__ Pre load(int f, size_t g) const
+    {
+        const size_t i = g - (size_t)f * Vn;
+        if (f < nm) return Pre{w0[(size_t)f * Vn + i]};
+        return Pre{elec ? p0[i] : mkc<V>(T(0), T(0))};
+    }
+    __device__ __forceinline__ V apply(int f, int, int, int, size_t g, V v, const Pre& p)
+    {
+        const size_t i = g - (size_t)f * Vn;
+        const V r = (f < nm || elec) ? cadd(p.b, v) : mkc<V>(T(0), T(0));
+        if (f < nm) w1[(size_t)f * Vn + i] = r;
+        else p1[i] = r;
+        if (!(isfinite((double)r.x) && isfinite((double)r.y))) bad += 1.0;
+        return r;
+    }
+    __device__ __forceinline__ void end(double* scratch, size_t cta)
+    {
+        if (!npart) return;
+        double v[1] = {bad};
+        __syncthreads();
+        block_sum<1>(v, scratch);
+        if (threadIdx.x == 0) npart[cta] = v[0];
+    }
 };
 
 // Stores the pass's values (a pass with no second transform).
@@ -732,6 +868,7 @@ struct Engine : EngineBase {
         pair_ix.release(); pair_wt.release(); pair_run.release();
         si_G.release(); si_inc.release(); ck.release();
         avg.acc.release();
+        upart.release();
         learn_release();
         if (ds) cudaFree(ds);
         release_events();
@@ -1167,6 +1304,73 @@ struct Engine : EngineBase {
             inc[i] = cscale(k, invV);
         }, (double)(2 * sizeof(V) + sizeof(T)));
         fft3<+1>(si_inc.p, nf);
+    }
+
+    // The whole semi-implicit update of the predictor (corr = false) or the
+    // corrector in three transform passes (grids with the plane pass): the
+    // increments are computed as the loads of the forward yz pass
+    // (OpIncrement, with the drift maxima of the corrector), the x pass
+    // applies P(k) and removes the psi increment's k = 0 value, and the
+    // inverse yz pass adds the increments to the fields (OpUpdate, with the
+    // corrector's non-finite count).  Removing the mean of the psi increment
+    // in k-space replaces the real-space mean removal of the updated psi
+    // (complexLangevin.cu:313-317): psi keeps the zero mean it was given
+    // (set_fields), up to rounding, and the physics does not depend on it.
+    Buf<double> upart;   // per-CTA drift maxima and non-finite counts of the fused update
+
+    void si_update_fused(bool corr, bool stash)
+    {
+        const size_t Vn = V_;
+        const int nm = c.nm, nf = nm + 1;
+        const size_t nparts = (size_t)c.m1 * nf;
+        if (!upart.p) upart.alloc(2 * nparts);
+        cudaEvent_t ev = prof_begin();
+        if (corr) {
+            OpIncrement<T, true> op{};
+            op.u0 = drift.p; op.u1 = drift_bar.p; op.e = eta.p; op.dp = dpsi.p; op.db = dpsi_bar.p; op.d = ds;
+            for (int a = 0; a < nm; ++a) op.co.s[a] = -0.5 * c.dt * c.lambda[a];
+            op.sp = -0.5 * c.dt * c.lpsi;
+            op.invV = 1.0 / (double)Vn; op.Vn = Vn; op.nm = nm; op.elec = c.elec; op.dpart = upart.p;
+            plane<0, -1>(nullptr, si_inc.p, nf, op);
+        } else {
+            OpIncrement<T, false> op{};
+            op.u0 = drift.p; op.e = eta.p; op.dp = dpsi.p; op.d = ds;
+            for (int a = 0; a < nm; ++a) op.co.s[a] = -c.dt * c.lambda[a];
+            op.sp = -c.dt * c.lpsi;
+            op.invV = 1.0 / (double)Vn; op.Vn = Vn; op.nm = nm; op.elec = c.elec;
+            plane<0, -1>(nullptr, si_inc.p, nf, op);
+        }
+        OpPrecond<T> pr{};
+        pr.GA = si_G.p;
+        pr.GL = lr.on_use ? lr.GL.p : nullptr;
+        pr.dw = stash ? lr.dw.p : nullptr;
+        pr.d = ds;
+        for (int a = 0; a < nm; ++a) pr.st.s[a] = c.dt * c.lambda[a];
+        pr.st.s[nm] = c.dt * c.lpsi;
+        pr.invV = (T)(1.0 / (double)Vn);
+        pr.dc0 = c.elec ? nm : -1;
+        strided<0, -1, +1>(si_inc.p, si_inc.p, nf, pr);
+        OpUpdate<T> up{};
+        up.w0 = corr ? omega.p : omega.p;
+        up.p0 = psi.p;
+        up.w1 = corr ? omega.p : omega_bar.p;
+        up.p1 = corr ? psi.p : psi_bar.p;
+        up.Vn = Vn; up.nm = nm; up.elec = c.elec;
+        up.npart = corr ? upart.p + nparts : nullptr;
+        plane<+1, 0>(si_inc.p, nullptr, nf, up);
+        // loads: drifts, noise (real), psi drift read and written; three
+        // passes over the increments; the fields read and written
+        const double units = corr ? (2.0 * nm + 0.5 * nf + 3.0 + nf) + 2.5 * nf + 3.0 * nf
+                                  : (1.0 * nm + 0.5 * nf + 2.5 + nf) + 2.5 * nf + 3.0 * nf;
+        prof_end(ev, "field_fft", units * sizeof(V) * (double)Vn);
+        if (corr) {
+            for (int f = 0; f < nf; ++f) {
+                k_combine<true><<<1, COMBINE_THREADS, 0, stream>>>(upart.p + (size_t)f * c.m1, c.m1, 1, ds->dmax + f);
+                ++launches;
+            }
+            k_combine<false><<<1, COMBINE_THREADS, 0, stream>>>(upart.p + nparts, (int)nparts, 1, ds->corr + 2);
+            ++launches;
+        }
     }
 
     // ---- learned semi-implicit preconditioner (learned.cuh) ----
@@ -2587,6 +2791,10 @@ struct Engine : EngineBase {
         T* e = eta.p;
         DevScal* d = ds;
         const double invV = 1.0 / (double)Vn;
+        if (c.scheme == FTSP_SCHEME_SI && plane_ok) {
+            si_update_fused(false, lr.on_collect || lr.on_use);
+            return;
+        }
         if (c.scheme == FTSP_SCHEME_SI) {
             V* inc = si_inc.p;
             foreach(Vn, [=] __device__(size_t i) {
@@ -2678,6 +2886,10 @@ struct Engine : EngineBase {
         const T* e = eta.p;
         DevScal* d = ds;
         const double invV = 1.0 / (double)Vn;
+        if (c.scheme == FTSP_SCHEME_SI && plane_ok) {
+            si_update_fused(true, false);
+            return;
+        }
         // drift maxima: max |u + u_bar|^2 per mode and for psi
         reduce<MAXMODE + 1, true>(Vn, [=] __device__(size_t i, double* acc) {
             for (int a = 0; a < nm; ++a) {
