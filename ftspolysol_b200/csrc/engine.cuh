@@ -2760,17 +2760,21 @@ struct Engine : EngineBase {
             // with fresh noise
             const uint64_t seed = c.seed;
             const DevScal* d = ds;
-            foreach(Vn, [=] __device__(size_t i) {
+            // the psi noise is summed as it is drawn (its mean is removed by
+            // the predictor, remove_real_mean, complexLangevin.cu:296)
+            reduce<1>(Vn, [=] __device__(size_t i, double* acc) {
                 const uint64_t st = d->step;
-                for (int f = 0; f <= nm; ++f)
-                    e[(size_t)f * Vn + i] = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
-            }, (double)(c.nm + 1) * sizeof(T));
-        }
-        noise_injected = false;
-        if (c.elec) {   // remove_real_mean of the psi noise (complexLangevin.cu:296)
+                for (int f = 0; f <= nm; ++f) {
+                    const T v = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
+                    e[(size_t)f * Vn + i] = v;
+                    if (f == nm) acc[0] += (double)v;
+                }
+            }, &ds->mean_eta, (double)(c.nm + 1) * sizeof(T));
+        } else if (c.elec) {   // injected noise: remove_real_mean of its psi part (complexLangevin.cu:296)
             const T* ep = e + (size_t)nm * Vn;
             reduce<1>(Vn, [=] __device__(size_t i, double* acc) { acc[0] += (double)ep[i]; }, &ds->mean_eta, (double)sizeof(T));
         }
+        noise_injected = false;
     }
 
     // ---- predictor (complexLangevin.cu:328-347) ----
