@@ -2997,7 +2997,10 @@ struct Engine : EngineBase {
         const int sum_m = m1 + m2 + m3;
         const DevScal* d = ds;
         const bool common = ion_common;
-        reduce<26>(Vn, [=] __device__(size_t i, double* acc) {
+        // two reductions: the density-field channels (0..13) and the
+        // electrostatic field term k_a k_b Psi(k) Psi(-k) (14..25), so that
+        // neither kernel holds all 26 FP64 accumulators
+        reduce<14>(Vn, [=] __device__(size_t i, double* acc) {
             const int x = (int)(i / ((size_t)m2 * m3));
             const int r = (int)(i - (size_t)x * m2 * m3);
             const int y = r / m3, z = r - y * m3;
@@ -3013,10 +3016,9 @@ struct Engine : EngineBase {
                 for (int a = 0; a < nm; ++a) w = dadd(w, dmul(to_d(kAp[(size_t)a * Vn + i]), oc.g[a * M + al]));
                 A = dadd(A, dmul(to_d(dBp[(size_t)al * Vn + ineg]), dscale(w, Gk)));
             }
-            double2 Bc = make_double2(0.0, 0.0), Ij = make_double2(0.0, 0.0), I0 = make_double2(0.0, 0.0), X = make_double2(0.0, 0.0);
+            double2 Bc = make_double2(0.0, 0.0), Ij = make_double2(0.0, 0.0), I0 = make_double2(0.0, 0.0);
             if (elec) {
                 const double2 Pk = to_d(kAp[(size_t)nm * Vn + i]);
-                const double2 Pm = to_d(kAp[(size_t)nm * Vn + ineg]);
                 const double2 rc = dmul(to_d(dBp[(size_t)M * Vn + ineg]), dscale(Pk, Gk));
                 Bc = make_double2(-rc.y, rc.x);   // i * R_c(-k) Gamma Psi(k)
                 if (common) {
@@ -3035,18 +3037,33 @@ struct Engine : EngineBase {
                         I0 = dadd(I0, dscale(ip, 1.0 / 6.0));
                     }
                 }
-                X = dmul(Pk, Pm);
             }
             const double2 base = make_double2(-a2 * (A.x + Bc.x) + Ij.x, -a2 * (A.y + Bc.y) + Ij.y);
             for (int cc = 0; cc < 6; ++cc) {
                 acc[2 * cc] += kk[cc] * base.x;
                 acc[2 * cc + 1] += kk[cc] * base.y;
-                acc[14 + 2 * cc] += kk[cc] * X.x;
-                acc[14 + 2 * cc + 1] += kk[cc] * X.y;
             }
             acc[12] += 0.5 * A.x + Bc.x / 6.0 + I0.x;
             acc[13] += 0.5 * A.y + Bc.y / 6.0 + I0.y;
-        }, ds->kobs, (double)(c.nm + c.M + 2 + (ion_common ? 1 : (int)c.ions.size())) * sizeof(V));
+        }, ds->kobs, (double)(c.nm + c.M + 1 + (ion_common ? 1 : (int)c.ions.size())) * sizeof(V));
+        if (!elec) {
+            FTSP_CUDA(cudaMemsetAsync(ds->kobs + 14, 0, 12 * sizeof(double), stream));
+            return;
+        }
+        reduce<12>(Vn, [=] __device__(size_t i, double* acc) {
+            const int x = (int)(i / ((size_t)m2 * m3));
+            const int r = (int)(i - (size_t)x * m2 * m3);
+            const int y = r / m3, z = r - y * m3;
+            const int nx = x ? m1 - x : 0, ny = y ? m2 - y : 0, nz = z ? m3 - z : 0;
+            const size_t ineg = ((size_t)nx * m2 + ny) * m3 + nz;
+            const double ax = kxp[x], ay = kyp[y], az = kzp[z];
+            const double kk[6] = {ax * ax, ay * ay, az * az, ax * ay, ax * az, ay * az};
+            const double2 X = dmul(to_d(kAp[(size_t)nm * Vn + i]), to_d(kAp[(size_t)nm * Vn + ineg]));
+            for (int cc = 0; cc < 6; ++cc) {
+                acc[2 * cc] += kk[cc] * X.x;
+                acc[2 * cc + 1] += kk[cc] * X.y;
+            }
+        }, ds->kobs + 14, 2.0 * sizeof(V));
     }
 
     void finalize_record(bool with_stress)
