@@ -951,6 +951,9 @@ struct Engine : EngineBase {
         const size_t nmv = Vn * std::max(1, nm);
         omega.alloc(nmv); omega_bar.alloc(nmv); drift.alloc(nmv); drift_bar.alloc(nmv);
         psi.alloc(Vn); psi_bar.alloc(Vn); dpsi.alloc(Vn); dpsi_bar.alloc(Vn);
+        // partials of the fused semi-implicit update (allocated here: a step
+        // may run under stream capture, where nothing can be allocated)
+        if (c.scheme == FTSP_SCHEME_SI) upart.alloc(2 * (size_t)c.m1 * (nm + 1));
         eta.alloc((size_t)(nm + 1) * Vn);
         kA.alloc((size_t)(nm + 1) * Vn);
         kB.alloc((size_t)(M + 1 + J) * Vn);
@@ -1323,7 +1326,6 @@ struct Engine : EngineBase {
         const size_t Vn = V_;
         const int nm = c.nm, nf = nm + 1;
         const size_t nparts = (size_t)c.m1 * nf;
-        if (!upart.p) upart.alloc(2 * nparts);
         cudaEvent_t ev = prof_begin();
         if (corr) {
             OpIncrement<T, true> op{};
