@@ -62,6 +62,10 @@ def parse_args():
                          "w2 = the 64^3 N=50 monovalent system")
     ap.add_argument("--ttp-dts", type=lambda x: [float(v) for v in x.split(",")], default=[0.01, 0.02],
                     help="step sizes of the complex64 plain and learned runs (comma separated)")
+    ap.add_argument("--ttp-checkpoint-every", type=int, default=100,
+                    help="device checkpoint interval of the time-to-Pi runs (the reference's Ntmp)")
+    ap.add_argument("--ttp-max-restarts", type=int, default=1000,
+                    help="rollbacks allowed in a time-to-Pi run (the reference's max_nan_restarts)")
     ap.add_argument("--ttp-train-steps", type=int, default=2000,
                     help="plain semi-implicit steps whose statistics train the network")
     ap.add_argument("--replicas", type=int, default=0,
@@ -160,8 +164,8 @@ def step_roofline(prop_bytes, field, steps, npts, s_c, steps_per_s_gpu, peak):
     achieved = total * steps_per_s_gpu / 1e9
     return {"bytes_per_step": total, "propagator_bytes_per_step": pbytes, "field_bytes_per_step": fbytes,
             "K_f": fbytes / (npts * s_c), "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
-            "field_kinds": {k: {"launches": v["launches"] / steps, "bytes": v["bytes"] / steps}
-                            for k, v in sorted(field.items())}}
+            "field_kinds": {k: {"launches": v["launches"] / steps, "bytes": v["bytes"] / steps,
+                                "ms_per_step": v["ms"] / steps} for k, v in sorted(field.items())}}
 
 
 def committed_traffic():
@@ -613,27 +617,44 @@ def run_ours(args, ws, rank, local):
 # ---------------------------------------------------------------------------
 # time to Pi: learned complex64 SI at dt = 0.02 against the plain runs
 # ---------------------------------------------------------------------------
-def _trajectory(eng, steps, t_wall0, rows, sim0, dt, idx):
-    """Steps with a synchronous record each; rows get (wall s, sim time, Pi,
+class _Trajectory:
+    """Synchronous steps with a record each; rows get (wall s, sim time, Pi,
     mu, mu_ex), mu being the polymer's total chemical potential
     mu_ex + mu_self + mu_id (record entries idx).  A non-finite step is
-    rolled back by the device on the next step (at most max_restarts times);
-    once the cap is reached the run is over and the trajectory stops.
-    Returns (non-finite steps, stopped)."""
-    import time
-    from ftspolysol_b200.engine import NonFinite
-    bad = 0
-    for k in range(steps):
-        try:
-            _, rec, _ = eng.step()
+    rolled back by the device on the next step to the last checkpoint (taken
+    after every `every`-th step attempt that ends finite); the rows of the
+    steps it undoes are dropped and the simulated time rewinds, as the
+    reference rewrites its observable file after a restart
+    (complexLangevin.cu:638-656).  After max_restarts rollbacks the run is
+    over and `stopped` is set."""
+
+    def __init__(self, eng, every, idx, t0):
+        self.eng, self.every, self.idx, self.t0 = eng, every, idx, t0
+        self.rows, self.attempts, self.ckpt_row, self.ckpt_sim = [], 0, 0, 0.0
+        self.sim, self.bad, self.stopped = 0.0, 0, False
+
+    def run(self, steps, dt):
+        import time
+        from ftspolysol_b200.engine import NonFinite
+        for _ in range(steps):
+            if self.stopped:
+                return
+            self.attempts += 1
+            try:
+                _, rec, _ = self.eng.step()
+            except NonFinite:
+                self.bad += 1
+                del self.rows[self.ckpt_row:]
+                self.sim = self.ckpt_sim
+                if self.eng.rollback_exhausted():
+                    self.stopped = True
+                continue
             r = rec.real
-            rows.append((time.perf_counter() - t_wall0, sim0 + (k + 1) * dt, r[-1], r[idx[0]] + r[idx[1]] + r[idx[2]],
-                         r[idx[0]]))
-        except NonFinite:
-            bad += 1
-            if eng.rollback_exhausted():
-                return bad, True
-    return bad, False
+            self.sim += dt
+            self.rows.append((time.perf_counter() - self.t0, self.sim, r[-1],
+                              r[self.idx[0]] + r[self.idx[1]] + r[self.idx[2]], r[self.idx[0]]))
+            if self.attempts % self.every == 0:
+                self.ckpt_row, self.ckpt_sim = len(self.rows), self.sim
 
 
 def _time_to_target(rows, target, tol=0.01, every=50):
@@ -686,52 +707,54 @@ def run_time_to_pi(args, local):
     N = len(case.species[0].monomers)
     runs = {}
 
-    def plain(prec, dt, tag):
+    every, cap = args.ttp_checkpoint_every, args.ttp_max_restarts
+
+    def engine(prec, dt):
         e = Engine(dict(d, dt=dt), precision=prec, scheme=SCHEME_SI, noise=True, seed=21, device=local,
-                   restart_interval=20)
+                   restart_interval=every, max_restarts=cap)
         e.set_fields(om, ps)
+        if args.adaptive > 0:
+            e.set_adaptive(args.adaptive)
         torch.cuda.synchronize()
-        rows = []
-        t0 = time.perf_counter()
-        bad, stopped = _trajectory(e, int(round(T / dt)), t0, rows, 0.0, dt, idx)
-        runs[tag] = {"rows": rows, "dt": dt, "nonfinite_steps": bad, "restarts": e.restarts(),
-                     "stopped_at_cap": stopped, "wall_s": rows[-1][0] if rows else None}
+        return e
+
+    def plain(prec, dt, tag):
+        e = engine(prec, dt)
+        tr = _Trajectory(e, every, idx, time.perf_counter())
+        limit = 4 * int(round(T / dt))   # step attempts, rolled-back ones included
+        while tr.sim < T - 0.5 * dt and not tr.stopped and tr.attempts < limit:
+            tr.run(min(int(round((T - tr.sim) / dt)), limit - tr.attempts), dt)
+        runs[tag] = {"rows": tr.rows, "dt": dt, "nonfinite_steps": tr.bad, "restarts": e.restarts(),
+                     "stopped_at_cap": tr.stopped, "attempts": tr.attempts,
+                     "wall_s": tr.rows[-1][0] if tr.rows else None}
         e.close()
 
     def learned(dt, tag):
         # plain SI steps at dt = 0.005 collect the statistics, Adam trains the
         # network, then steps of dt with the learned kernel, retrained online
-        e = Engine(dict(d, dt=0.005), precision=FP32, scheme=SCHEME_SI, noise=True, seed=21, device=local,
-                   restart_interval=20)
-        e.set_fields(om, ps)
+        e = engine(FP32, 0.005)
         e.learn_configure(N=N, lB=case.lB, salt=salt, seed=11)
-        torch.cuda.synchronize()
-        rows = []
-        t0 = time.perf_counter()
+        tr = _Trajectory(e, every, idx, time.perf_counter())
         ntrain = min(args.ttp_train_steps, int(round(T / 0.005)) // 2)
         e.learn_collect(True)
-        bad, stopped = _trajectory(e, ntrain, t0, rows, 0.0, 0.005, idx)
-        loss = e.learn_train(1500) if not stopped else None
+        tr.run(ntrain, 0.005)
+        loss = e.learn_train(1500) if not tr.stopped else None
         valid = e.learn_stats()["valid_targets"]
-        t_train = time.perf_counter() - t0
-        if not stopped:
+        t_train = time.perf_counter() - tr.t0
+        if not tr.stopped:
             e.set_dt(dt)
             e.learn_use(True)
             e.learn_reset()
-        sim = ntrain * 0.005
-        nbig = int(round((T - sim) / dt))
-        done = 0
-        while done < nbig and not stopped:
-            k = min(200, nbig - done)
-            b, stopped = _trajectory(e, k, t0, rows, sim + done * dt, dt, idx)
-            bad += b
-            done += k
-            if not stopped:
+        limit = tr.attempts + 4 * int(round((T - tr.sim) / dt))
+        while tr.sim < T - 0.5 * dt and not tr.stopped and tr.attempts < limit:
+            tr.run(min(200, int(round((T - tr.sim) / dt)), limit - tr.attempts), dt)
+            if not tr.stopped:
                 e.learn_train(200)
                 e.learn_reset()
         st = e.learn_stats()
-        runs[tag] = {"rows": rows, "dt": dt, "nonfinite_steps": bad, "restarts": e.restarts(), "stopped_at_cap": stopped,
-                     "wall_s": rows[-1][0] if rows else None, "train_steps": ntrain, "train_wall_s": t_train,
+        runs[tag] = {"rows": tr.rows, "dt": dt, "nonfinite_steps": tr.bad, "restarts": e.restarts(),
+                     "stopped_at_cap": tr.stopped, "attempts": tr.attempts,
+                     "wall_s": tr.rows[-1][0] if tr.rows else None, "train_steps": ntrain, "train_wall_s": t_train,
                      "train_loss": loss, "valid_targets": valid, "fallback_steps": st["fallbacks"],
                      "judged_steps": st["checks"]}
         e.close()
@@ -779,6 +802,8 @@ def run_time_to_pi(args, local):
                                    "stay within 1% of the target from then on; mu = mu_ex + mu_self + mu_id of the "
                                    "polymer (mu_ex alone averages near zero: its absolute error is reported)",
                       "simulated_time": T,
+                      "rollback": {"checkpoint_every": every, "max_restarts": cap,
+                                   "adaptive_u_ref": args.adaptive or None},
                       "config": {"workload": case.name + ": %d^3, L=%gb, N=%d, %s counterions, salt %g"
                                  % (case.m[0], case.L[0], N,
                                     "divalent" if case.counterions["valence"] == 2.0 else "monovalent", salt)},

@@ -68,7 +68,8 @@ struct DevScal {
     alignas(16) double rec[2 * 128];
     alignas(16) unsigned long long step;   // steps taken: keys the noise, schedules the checkpoints
     long long avg_seen;                    // time averaging: steps since ftsp_average_start
-    long long avg_count;                   // of those, records accumulated
+    long long avg_count;                   // of those, records accumulated (committed + pending)
+    long long avg_committed;               // records in the blocks (past a checkpoint)
     alignas(16) double dt_scale;           // this step's dt / configured dt (1 unless the step is adaptive)
     double umax;                           // max |drift| at the start of this step (adaptive step)
     alignas(16) double lres[2];            // learned preconditioner: force residuals (learned, analytic) of the step
@@ -221,29 +222,48 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
 // Fixed-order combine of `count` partial rows of K channels: one warp per
 // channel (grid K), lanes stride over the rows, then a shuffle tree.
 // Time averaging of the observable record (complexLangevin.cu:424-441): a
-// step's record is accumulated when more than `skip` steps have been seen
-// since the averaging started, fewer than `samples` records have been
-// accumulated and the step is finite; the real part of every entry, weighted
-// by the step's dt scale (1 unless the step is adaptive), into block
-// avg_count / per_block.  acc holds per block R weighted sums, the weight sum
+// step's record is taken when more than `skip` steps have been seen since
+// the averaging started, fewer than `samples` records have been taken and
+// the step is finite; the real part of every entry, weighted by the step's
+// dt scale (1 unless the step is adaptive).  Records first go to a pending
+// accumulator (acc + nblk * (R + 2)); the pending records are committed to
+// block avg_committed / per_block when the step is a checkpoint (every
+// `every` steps, or every step without rollback) and discarded by a
+// rollback, which restores the checkpoint (restore_if_bad), so the averages
+// hold exactly the records of the trajectory that was kept, as the
+// reference rewrites its observable file after a restart
+// (complexLangevin.cu:638-656).  Per block: R weighted sums, the weight sum
 // and the record count.  One CTA; the counters move after every thread has
 // read them.
-static __global__ void k_average(DevScal* d, double* acc, int R, long long skip, long long samples, long long per_block)
+static __global__ void k_average(DevScal* d, double* acc, int R, int nblk, long long skip, long long samples,
+                                 long long per_block, unsigned long long every)
 {
+    double* pend = acc + (size_t)nblk * (R + 2);
     const bool take = d->avg_seen + 1 > skip && d->avg_count < samples && !d->bad_last;
     if (take) {
-        double* a = acc + (size_t)(d->avg_count / per_block) * (R + 2);
         const double w = d->dt_scale;
-        for (int i = threadIdx.x; i < R; i += blockDim.x) a[i] += w * d->rec[2 * i];
+        for (int i = threadIdx.x; i < R; i += blockDim.x) pend[i] += w * d->rec[2 * i];
         if (threadIdx.x == 0) {
-            a[R] += w;
-            a[R + 1] += 1.0;
+            pend[R] += w;
+            pend[R + 1] += 1.0;
+        }
+    }
+    __syncthreads();
+    const bool commit = !d->bad_last && (every == 0 || d->step % every == 0);
+    const double pn = pend[R + 1];
+    if (commit && pn > 0.0) {
+        const long long b = d->avg_committed / per_block;
+        double* a = acc + (size_t)(b < nblk ? b : nblk - 1) * (R + 2);
+        for (int i = threadIdx.x; i < R + 2; i += blockDim.x) {
+            a[i] += pend[i];
+            pend[i] = 0.0;
         }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         d->avg_seen += 1;
         if (take) d->avg_count += 1;
+        if (commit && pn > 0.0) d->avg_committed += (long long)pn;
     }
 }
 
@@ -1927,8 +1947,9 @@ struct Engine : EngineBase {
         if constexpr (S1 != 0 && S2 != 0 && F32 && N == 128 && NT == 1024 && op_loads<Op>::value <= 1) {
             if (zreg_plane) {
                 auto k = k_plane_zreg<T, S1, S2, Op>;
-                set_smem(k, smem);
-                launch_pass(k, dim3(c.m1, nf), NT, smem, src, dst, (size_t)V_, (const V*)tw3.p, op);
+                const size_t zsmem = smem + sizeof(V) * 128;   // + the [t][i] twiddle table
+                set_smem(k, zsmem);
+                launch_pass(k, dim3(c.m1, nf), NT, zsmem, src, dst, (size_t)V_, (const V*)tw3.p, op);
                 ++launches;
                 return;
             }
@@ -3483,6 +3504,8 @@ struct Engine : EngineBase {
             for (int a = 0; a < nm; ++a) om[(size_t)a * Vn + i] = ckp[(size_t)a * Vn + i];
             ps[i] = ckp[(size_t)nm * Vn + i];
         });
+        double* pend = avg.on ? avg.acc.p + (size_t)avg.nblk * (c.record_len() + 2) : nullptr;
+        const int R2 = c.record_len() + 2;
         k_foreach<<<1, 32, 0, stream>>>(1, [=] __device__(size_t) {
             if (d->bad_last && !d->exhausted) {
                 if (d->restarts >= cap) {
@@ -3490,6 +3513,10 @@ struct Engine : EngineBase {
                 } else {
                     d->restarts += 1;
                     d->bad_last = 0;
+                    if (pend) {   // the records since the checkpoint are undone with the fields
+                        d->avg_count -= (long long)pend[R2 - 1];
+                        for (int i = 0; i < R2; ++i) pend[i] = 0.0;
+                    }
                 }
             }
         });
@@ -3558,7 +3585,8 @@ struct Engine : EngineBase {
         if (learn) learn_after_step();
         mark_step_status();
         if (avg.on) {
-            k_average<<<1, 128, 0, stream>>>(ds, avg.acc.p, c.record_len(), avg.skip, avg.samples, avg.per_block);
+            k_average<<<1, 128, 0, stream>>>(ds, avg.acc.p, c.record_len(), avg.nblk, avg.skip, avg.samples,
+                                             avg.per_block, (unsigned long long)c.restart_interval);
             ++launches;
         }
         if (c.restart_interval > 0) checkpoint_if_good();
@@ -3568,8 +3596,8 @@ struct Engine : EngineBase {
     struct Avg {
         bool on = false;
         long long skip = 0, samples = 0, per_block = 1;
-        int blocks = 0;
-        Buf<double> acc;
+        int blocks = 0, nblk = 0;
+        Buf<double> acc;   // nblk blocks of (R + 2), then the pending accumulator
     } avg;
 
     void average_start(long long skip, long long samples, int blocks) override
@@ -3584,10 +3612,10 @@ struct Engine : EngineBase {
         avg.blocks = blocks;
         avg.per_block = (samples + blocks - 1) / blocks;
         const int R = c.record_len();
-        const int nblk = (int)((samples + avg.per_block - 1) / avg.per_block);
-        avg.acc.alloc((size_t)nblk * (R + 2));
+        avg.nblk = (int)((samples + avg.per_block - 1) / avg.per_block);
+        avg.acc.alloc((size_t)(avg.nblk + 1) * (R + 2));
         FTSP_CUDA(cudaMemsetAsync(avg.acc.p, 0, sizeof(double) * avg.acc.n, stream));
-        FTSP_CUDA(cudaMemsetAsync(&ds->avg_seen, 0, 2 * sizeof(long long), stream));
+        FTSP_CUDA(cudaMemsetAsync(&ds->avg_seen, 0, 3 * sizeof(long long), stream));
         FTSP_CUDA(cudaStreamSynchronize(stream));
         avg.on = true;
     }
@@ -3602,7 +3630,7 @@ struct Engine : EngineBase {
         std::vector<double> a(avg.acc.n);
         FTSP_CUDA(cudaMemcpyAsync(a.data(), avg.acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, stream));
         pull_scalars();
-        const int nblk = (int)(a.size() / (R + 2));
+        const int nblk = avg.nblk;
         std::vector<double> sum(R, 0.0);
         double wsum = 0.0;
         std::vector<std::vector<double>> bm;
@@ -3631,7 +3659,7 @@ struct Engine : EngineBase {
                 se[i] = std::sqrt(v / (double)(bm.size() - 1) / (double)bm.size());
             }
         }
-        return hs.avg_count;
+        return hs.avg_committed;
     }
 
     int status_from_host()

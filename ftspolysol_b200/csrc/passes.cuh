@@ -1208,11 +1208,16 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
     V* stw = tile + N * P;
+    // twiddles w^(t i) of the register-resident z stage laid out [t][i]
+    // (t < 8, i < 16): its 16 consecutive threads take 16 consecutive
+    // entries, where the plain table would serve them with bank conflicts
+    V* stz = stw + N;
     const int tid = threadIdx.x;
     const int x = blockIdx.x;
     const int f = blockIdx.y;
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     for (int j = tid; j < N; j += 1024) stw[j] = twn[j];
+    if (tid < 128) stz[tid] = twn[(tid >> 4) * (tid & 15)];
     if (tid == 0) op.prefetch(base, (unsigned)NE);   // L2 prefetch: cannot observe a stale value
     pdl_wait();
     const int zc = tid & 127;   // column of the y-stages
@@ -1273,7 +1278,15 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int y = (tid >> 4) + 64 * q;
-            bfly_k<S1, 8>(u[q], i, stw);
+            if (i) {
+#pragma unroll
+                for (int t = 1; t < 8; ++t) {
+                    V w = stz[t * 16 + i];
+                    if (S1 > 0) w.y = -w.y;
+                    u[q][t] = cmul(u[q][t], w);
+                }
+            }
+            dftR<S1, 8>(u[q]);
             typename Op::Pre pre[8];
 #pragma unroll
             for (int t = 0; t < 8; ++t) pre[t] = op.load(f, base + (size_t)y * N + i + 16 * t);

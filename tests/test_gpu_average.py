@@ -63,3 +63,37 @@ def test_average_in_a_replica_batch():
     assert na == nb == 12
     np.testing.assert_array_equal(ma, mb)
     np.testing.assert_array_equal(sa, sb)
+
+
+def test_average_drops_records_undone_by_a_rollback():
+    """A non-finite step rolls the fields back to the last checkpoint; the
+    records taken since that checkpoint go with them, and only records up to
+    the last checkpoint are committed to the averages."""
+    from ftspolysol_b200 import Engine, FP64, SCHEME_SI
+    from ftspolysol_b200.engine import NonFinite
+    case = workload(1)
+    d = derive(case)
+    om, ps = case.initial_fields()
+    every = 4
+    e = Engine(d, precision=FP64, scheme=SCHEME_SI, noise=True, seed=9, restart_interval=every)
+    e.set_fields(om, ps)
+    e.average_start(0, 1000, 2)
+    nan_eta = np.zeros((2, case.size))
+    nan_eta[0, 5] = np.nan
+    rows, ckpt = [], 0
+    for attempt in range(1, 15):
+        if attempt in (7, 10):
+            e.set_noise(nan_eta)
+        try:
+            _, rec, _ = e.step()
+        except NonFinite:
+            del rows[ckpt:]
+            continue
+        rows.append(rec.real.copy())
+        if attempt % every == 0:
+            ckpt = len(rows)
+    mean, _, n = e.average_read()
+    e.close()
+    kept = np.array(rows[:ckpt])
+    assert n == len(kept)
+    np.testing.assert_allclose(mean, kept.mean(axis=0), rtol=1e-12, atol=1e-14)
