@@ -336,11 +336,11 @@ struct Renorm {
     int N;                   // segments of the species
 };
 
-__device__ __forceinline__ int reduce_exponent(const float* pm, int n)
+// the exponent floor(log2 max) of the previous pass's per-CTA maxima; m is
+// this thread's share of them (its strided elements), loaded beforehand
+__device__ __forceinline__ int reduce_exponent_local(float m)
 {
     __shared__ float s_red[32];
-    float m = 0.0f;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, pm[i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = m;
@@ -355,6 +355,15 @@ __device__ __forceinline__ int reduce_exponent(const float* pm, int n)
     __syncthreads();
     return (M > 0.0f && isfinite(M)) ? ilogbf(M) : 0;
 }
+
+__device__ __forceinline__ float local_max(const float* pm, int n)
+{
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, pm[i]);
+    return m;
+}
+
+__device__ __forceinline__ int reduce_exponent(const float* pm, int n) { return reduce_exponent_local(local_max(pm, n)); }
 
 // Chain-propagator pointwise work in the real-space pass of one segment.
 // KIND selects the sweep position:
@@ -389,6 +398,8 @@ struct OpProp {
     bool store_u;            // forward: store u = q / E (renormalised) instead of q
     double acc[2];
     float amax;
+    float pm_local;          // this thread's share of the previous maxima (preload)
+    bool preloaded;
     T fr, fi;                // density factor (with the segment's exponent folded in)
     T oscale;                // output scale 2^-d
 
@@ -402,6 +413,17 @@ struct OpProp {
         V e, q, r, c;
     };
 
+    // loads the previous pass's per-CTA maxima early (kernels that call it
+    // right after the dependency wait hide the latency behind their first
+    // transform stages; begin() reduces them)
+    __device__ __forceinline__ void preload()
+    {
+        preloaded = false;
+        if ((KIND == FWD_MID || KIND == FWD_LAST || KIND == BWD_MID) && rn.eF) {
+            pm_local = local_max(rn.pmax_prev, rn.nparts);
+            preloaded = true;
+        }
+    }
     __device__ __forceinline__ void begin()
     {
         acc[0] = acc[1] = 0.0;
@@ -413,13 +435,13 @@ struct OpProp {
             if (KIND == FWD_START || KIND == FWD_SINGLE) {
                 if (first) rn.eF[0] = 0;
             } else if (KIND == FWD_MID || KIND == FWD_LAST) {
-                const int d = reduce_exponent(rn.pmax_prev, rn.nparts);
+                const int d = preloaded ? reduce_exponent_local(pm_local) : reduce_exponent(rn.pmax_prev, rn.nparts);
                 oscale = (T)ldexp(1.0, -d);
                 if (first) rn.eF[rn.s] = rn.eF[rn.s - 1] + d;
             } else if (KIND == BWD_START || KIND == BWD_SINGLE) {
                 if (first) rn.eB[rn.s] = 0;
             } else if (KIND == BWD_MID) {
-                const int d = reduce_exponent(rn.pmax_prev, rn.nparts);
+                const int d = preloaded ? reduce_exponent_local(pm_local) : reduce_exponent(rn.pmax_prev, rn.nparts);
                 oscale = (T)ldexp(1.0, -d);
                 if (first) rn.eB[rn.s] = rn.eB[rn.s + 1] + d;
                 dens_exp = rn.eF[rn.s] + rn.eB[rn.s + 1] - rn.eF[rn.N - 1];
@@ -728,6 +750,7 @@ __global__ void __launch_bounds__(NT, 1) k_plane_fused(const cplx<T>* src, cplx<
     // table (the bulk of it) is not written during a sweep
     if (threadIdx.x == 0) op.prefetch(base, (unsigned)NE);
     pdl_wait();
+    op.preload();
     V v[E];   // value u: row tid/N + u*NT/N, column tid%N
 #pragma unroll
     for (int u = 0; u < E; ++u) v[u] = src[base + threadIdx.x + u * NT];
@@ -1220,6 +1243,7 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
     if (tid < 128) stz[tid] = twn[(tid >> 4) * (tid & 15)];
     if (tid == 0) op.prefetch(base, (unsigned)NE);   // L2 prefetch: cannot observe a stale value
     pdl_wait();
+    op.preload();
     const int zc = tid & 127;   // column of the y-stages
     const int hi = tid >> 7;    // 0..7
     // inverse y, stage 0 (radix 16, span 1): the coalesced load of column zc,
