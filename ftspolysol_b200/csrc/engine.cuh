@@ -495,54 +495,71 @@ struct OpIncrement {
     size_t Vn;
     int nm;
     bool elec;
-    double* dpart;           // corrector: per-CTA drift maxima [cta][nm + 1]
-    mutable double dmax;
+    double* dpart;           // corrector: per-CTA drift maxima
+    double dmax;
+    // the raw operands of a point; the loads carry no side effect, so a
+    // kernel keeps a whole batch of them in flight, and apply() does the
+    // arithmetic and the write-backs
     struct Pre {
-        V v;
+        V a, b;              // modes: u, u_bar; psi: psi drift, psi drift at the predictor
+        T e;
     };
     __device__ __forceinline__ void begin() { dmax = 0.0; }
     __device__ __forceinline__ Pre load(int f, size_t g) const
     {
         const size_t i = g - (size_t)f * Vn;
+        Pre p;
         if (f < nm) {
             const size_t j = (size_t)f * Vn + i;
-            V s = u0[j];
+            p.a = u0[j];
+            if (CORR) p.b = u1[j];
+            p.e = e[j];
+        } else if (elec) {
+            p.a = dp[i];
+            if (CORR) p.b = db[i];
+            p.e = e[(size_t)nm * Vn + i];
+        }
+        return p;
+    }
+    __device__ __forceinline__ V apply(int f, int, int, int, size_t g, V, const Pre& p)
+    {
+        const size_t i = g - (size_t)f * Vn;
+        if (f < nm) {
+            V s = p.a;
             if (CORR) {
-                s = cadd(s, u1[j]);
+                s = cadd(s, p.b);
                 double m = (double)s.x * s.x + (double)s.y * s.y;
                 if (!isfinite(m)) m = INFINITY;
                 dmax = fmax(dmax, m);
             }
             V v = cscale(s, (T)(co.s[f] * d->dt_scale));
-            v.x += e[j];
-            return Pre{v};
+            v.x += p.e;
+            return v;
         }
-        if (!elec) return Pre{mkc<V>(T(0), T(0))};
-        const size_t j = (size_t)nm * Vn + i;
-        T ep = e[j];
-        if (!CORR) {
-            ep = (T)((double)ep + (-(d->mean_eta * invV)));
-            e[j] = ep;
-        }
+        if (!elec) return mkc<V>(T(0), T(0));
+        T ep = p.e;
         // mean_dpsi: the sum of the psi drift of the last density evaluation
-        // (at omega, psi for the predictor; at the predictor's fields for the corrector)
+        // (at omega, psi for the predictor; at the predictor's fields for the
+        // corrector); the mean-removed values are written back, the corrector
+        // and the caller read them
         V s;
         if (!CORR) {
-            s = cadd(dp[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+            ep = (T)((double)ep + (-(d->mean_eta * invV)));
+            e[(size_t)nm * Vn + i] = ep;
+            s = cadd(p.a, from_d<V>(dscale(d->mean_dpsi, -invV)));
             dp[i] = s;
         } else {
-            const V dbv = cadd(db[i], from_d<V>(dscale(d->mean_dpsi, -invV)));
+            const V dbv = cadd(p.b, from_d<V>(dscale(d->mean_dpsi, -invV)));
             db[i] = dbv;
-            s = cadd(dp[i], dbv);
+            s = cadd(p.a, dbv);
             double m = (double)s.x * s.x + (double)s.y * s.y;
             if (!isfinite(m)) m = INFINITY;
             dmax = fmax(dmax, m);
         }
         V v = cscale(s, (T)(sp * d->dt_scale));
         v.x += ep;
-        return Pre{v};
+        return v;
     }
-    __device__ __forceinline__ V apply(int, int, int, int, size_t, V, const Pre& p) const { return p.v; }
     __device__ __forceinline__ void end(double* scratch, size_t cta)
     {
         if (!CORR) return;
@@ -1947,7 +1964,7 @@ struct Engine : EngineBase {
         if constexpr (S1 != 0 && S2 != 0 && F32 && N == 128 && NT == 1024 && op_loads<Op>::value <= 1) {
             if (zreg_plane) {
                 auto k = k_plane_zreg<T, S1, S2, Op>;
-                const size_t zsmem = smem + sizeof(V) * 128;   // + the [t][i] twiddle table
+                const size_t zsmem = smem + sizeof(V) * (128 + 64 * 128);   // + [t][i] twiddles, half the class table
                 set_smem(k, zsmem);
                 launch_pass(k, dim3(c.m1, nf), NT, zsmem, src, dst, (size_t)V_, (const V*)tw3.p, op);
                 ++launches;
