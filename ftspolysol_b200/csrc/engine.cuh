@@ -387,6 +387,19 @@ struct ModeTab {
 struct SigTab {
     double s[MAXMODE + 1];
 };
+
+// a[i] for a run-time i < K with constant indices only: an array in a
+// kernel's parameter block indexed at run time is copied to local memory
+// by every thread
+template <int K>
+__device__ __forceinline__ double pick(const double (&a)[K], int i)
+{
+    double v = a[0];
+#pragma unroll
+    for (int k = 1; k < K; ++k)
+        if (i == k) v = a[k];
+    return v;
+}
 struct SiOTab {
     double O[MAXMODE * MAXM];
 };
@@ -462,7 +475,7 @@ struct OpPrecond {
     __device__ __forceinline__ cplx<T> apply(int f, int x, int y, int z, size_t g, cplx<T> v, const Pre&) const
     {
         const T G = (GL && d->lr_use) ? GL[g] : GA[g];
-        const cplx<T> k = cscale(v, (T)(1.0 / (1.0 + (st.s[f] * d->dt_scale) * (double)G)));
+        const cplx<T> k = cscale(v, (T)(1.0 / (1.0 + (pick(st.s, f) * d->dt_scale) * (double)G)));
         if (dw) dw[g] = k;
         if (f == dc0 && (x | y | z) == 0) return mkc<cplx<T>>(T(0), T(0));
         return cscale(k, invV);
@@ -489,8 +502,7 @@ struct OpIncrement {
     V* dp;                   // psi drift at (omega, psi)
     V* db;                   // psi drift at (omega_bar, psi_bar) (corrector)
     const DevScal* d;
-    ModeTab co;              // c_f of the modes
-    double sp;               // c_f of psi
+    SigTab cs;               // c_f of the modes, then of psi
     double invV;
     size_t Vn;
     int nm;
@@ -532,7 +544,7 @@ struct OpIncrement {
                 if (!isfinite(m)) m = INFINITY;
                 dmax = fmax(dmax, m);
             }
-            V v = cscale(s, (T)(co.s[f] * d->dt_scale));
+            V v = cscale(s, (T)(pick(cs.s, f) * d->dt_scale));
             v.x += p.e;
             return v;
         }
@@ -556,7 +568,7 @@ struct OpIncrement {
             if (!isfinite(m)) m = INFINITY;
             dmax = fmax(dmax, m);
         }
-        V v = cscale(s, (T)(sp * d->dt_scale));
+        V v = cscale(s, (T)(pick(cs.s, nm) * d->dt_scale));
         v.x += ep;
         return v;
     }
@@ -1367,15 +1379,15 @@ struct Engine : EngineBase {
         if (corr) {
             OpIncrement<T, true> op{};
             op.u0 = drift.p; op.u1 = drift_bar.p; op.e = eta.p; op.dp = dpsi.p; op.db = dpsi_bar.p; op.d = ds;
-            for (int a = 0; a < nm; ++a) op.co.s[a] = -0.5 * c.dt * c.lambda[a];
-            op.sp = -0.5 * c.dt * c.lpsi;
+            for (int a = 0; a < nm; ++a) op.cs.s[a] = -0.5 * c.dt * c.lambda[a];
+            op.cs.s[nm] = -0.5 * c.dt * c.lpsi;
             op.invV = 1.0 / (double)Vn; op.Vn = Vn; op.nm = nm; op.elec = c.elec; op.dpart = upart.p;
             plane<0, -1>(nullptr, si_inc.p, nf, op);
         } else {
             OpIncrement<T, false> op{};
             op.u0 = drift.p; op.e = eta.p; op.dp = dpsi.p; op.d = ds;
-            for (int a = 0; a < nm; ++a) op.co.s[a] = -c.dt * c.lambda[a];
-            op.sp = -c.dt * c.lpsi;
+            for (int a = 0; a < nm; ++a) op.cs.s[a] = -c.dt * c.lambda[a];
+            op.cs.s[nm] = -c.dt * c.lpsi;
             op.invV = 1.0 / (double)Vn; op.Vn = Vn; op.nm = nm; op.elec = c.elec;
             plane<0, -1>(nullptr, si_inc.p, nf, op);
         }
@@ -1964,7 +1976,7 @@ struct Engine : EngineBase {
         if constexpr (S1 != 0 && S2 != 0 && F32 && N == 128 && NT == 1024 && op_loads<Op>::value <= 1) {
             if (zreg_plane) {
                 auto k = k_plane_zreg<T, S1, S2, Op>;
-                const size_t zsmem = smem + sizeof(V) * (128 + 64 * 128);   // + [t][i] twiddles, half the class table
+                const size_t zsmem = smem + sizeof(V) * 128;   // + the [t][i] twiddle table
                 set_smem(k, zsmem);
                 launch_pass(k, dim3(c.m1, nf), NT, zsmem, src, dst, (size_t)V_, (const V*)tw3.p, op);
                 ++launches;
@@ -2584,7 +2596,9 @@ struct Engine : EngineBase {
                         Ep[(size_t)k * Vn + i] = cexpT(-w.x, -w.y);
                     }
                     for (int al = 0; al <= M; ++al) dBp[(size_t)al * Vn + i] = mkc<V>(T(0), T(0));
-                    for (int j = 0; j < J; ++j) {
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {   // J <= 3 on this path
+                        if (j >= J) break;
                         const T zz = (T)zi.z[j];
                         const V b = cexpT(zz * ps_.y, -zz * ps_.x);
                         acc[2 * j] += (double)b.x;
@@ -2766,18 +2780,27 @@ struct Engine : EngineBase {
         const V* om = which ? omega_bar.p : omega.p;
         V* u = which ? drift_bar.p : drift.p;
         const V* rt = kC.p;
+        // gamma_a O_{a alpha} at a * MAXM + alpha: the loops below run to the
+        // compile-time maxima, so every table entry and accumulator has a
+        // constant index (no local-memory copies)
         ModeTab co{};
         for (int a = 0; a < nm; ++a) {
             co.c[a] = c.coeff[a];
             for (int al = 0; al < M; ++al)
-                co.g[a * M + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
+                co.g[a * MAXM + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
         }
         reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
-            for (int a = 0; a < nm; ++a) {
+#pragma unroll
+            for (int a = 0; a < MAXMODE; ++a) {
+                if (a >= nm) break;
                 const V w = om[(size_t)a * Vn + i];
                 // clear, add_scaled_complex(w, c), add_scaled_complex_const(rho, gamma O)
                 V v = cscale(w, (T)co.c[a]);
-                for (int al = 0; al < M; ++al) v = cadd(v, cmul(rt[(size_t)al * Vn + i], from_d<V>(co.g[a * M + al])));
+#pragma unroll
+                for (int al = 0; al < MAXM; ++al) {
+                    if (al >= M) break;
+                    v = cadd(v, cmul(rt[(size_t)al * Vn + i], from_d<V>(co.g[a * MAXM + al])));
+                }
                 u[(size_t)a * Vn + i] = v;
                 const double2 wd = to_d(w);
                 acc[2 * a] += wd.x * wd.x - wd.y * wd.y;
@@ -2804,7 +2827,9 @@ struct Engine : EngineBase {
             // the predictor, remove_real_mean, complexLangevin.cu:296)
             reduce<1>(Vn, [=] __device__(size_t i, double* acc) {
                 const uint64_t st = d->step;
-                for (int f = 0; f <= nm; ++f) {
+#pragma unroll
+                for (int f = 0; f <= MAXMODE; ++f) {
+                    if (f > nm) break;
                     const T v = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
                     e[(size_t)f * Vn + i] = v;
                     if (f == nm) acc[0] += (double)v;
@@ -2847,7 +2872,9 @@ struct Engine : EngineBase {
                     ep = (T)((double)ep + (-(d->mean_eta * invV)));
                     e[(size_t)nm * Vn + i] = ep;
                 }
-                for (int a = 0; a < nm; ++a) {
+#pragma unroll
+                for (int a = 0; a < MAXMODE; ++a) {
+                    if (a >= nm) break;
                     V v = cscale(u[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale));
                     v.x += e[(size_t)a * Vn + i];
                     inc[(size_t)a * Vn + i] = v;
@@ -2863,7 +2890,11 @@ struct Engine : EngineBase {
             }, (double)(c.nm * (2 * sizeof(V) + sizeof(T)) + 2 * sizeof(T) + 3 * sizeof(V)));
             si_precondition(lr.on_collect || lr.on_use);
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
-                for (int a = 0; a < nm; ++a) ob[(size_t)a * Vn + i] = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
+#pragma unroll
+                for (int a = 0; a < MAXMODE; ++a) {
+                    if (a >= nm) break;
+                    ob[(size_t)a * Vn + i] = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
+                }
                 const V pv = elec ? cadd(ps[i], inc[(size_t)nm * Vn + i]) : mkc<V>(T(0), T(0));
                 pb[i] = pv;
                 acc[0] += (double)pv.x;
@@ -2879,7 +2910,9 @@ struct Engine : EngineBase {
                 ep = (T)((double)ep + (-me));
                 e[(size_t)nm * Vn + i] = ep;
             }
-            for (int a = 0; a < nm; ++a) {
+#pragma unroll
+            for (int a = 0; a < MAXMODE; ++a) {
+                if (a >= nm) break;
                 V v = om[(size_t)a * Vn + i];
                 v = cadd(v, cscale(u[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
                 v.x += e[(size_t)a * Vn + i];
@@ -2936,7 +2969,9 @@ struct Engine : EngineBase {
         }
         // drift maxima: max |u + u_bar|^2 per mode and for psi
         reduce<MAXMODE + 1, true>(Vn, [=] __device__(size_t i, double* acc) {
-            for (int a = 0; a < nm; ++a) {
+#pragma unroll
+            for (int a = 0; a < MAXMODE; ++a) {
+                if (a >= nm) break;
                 const V s = cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]);
                 double v = (double)s.x * s.x + (double)s.y * s.y;
                 if (!isfinite(v)) v = INFINITY;
@@ -2947,12 +2982,16 @@ struct Engine : EngineBase {
             const V s = cadd(dp[i], dbv);
             double v = (double)s.x * s.x + (double)s.y * s.y;
             if (!isfinite(v)) v = INFINITY;
-            acc[nm] = fmax(acc[nm], v);
+#pragma unroll
+            for (int k = 0; k <= MAXMODE; ++k)   // acc[nm] with a constant index
+                if (k == nm) acc[k] = fmax(acc[k], v);
         }, ds->dmax, (double)(2 * c.nm + 2) * sizeof(V));
         if (c.scheme == FTSP_SCHEME_SI) {
             V* inc = si_inc.p;
             foreach(Vn, [=] __device__(size_t i) {
-                for (int a = 0; a < nm; ++a) {
+#pragma unroll
+                for (int a = 0; a < MAXMODE; ++a) {
+                    if (a >= nm) break;
                     V v = cscale(cadd(u0[(size_t)a * Vn + i], u1[(size_t)a * Vn + i]), (T)(co.s[a] * d->dt_scale));
                     v.x += e[(size_t)a * Vn + i];
                     inc[(size_t)a * Vn + i] = v;
@@ -2969,7 +3008,9 @@ struct Engine : EngineBase {
             si_precondition();
             reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
                 bool bad = false;
-                for (int a = 0; a < nm; ++a) {
+#pragma unroll
+                for (int a = 0; a < MAXMODE; ++a) {
+                    if (a >= nm) break;
                     const V w = cadd(om[(size_t)a * Vn + i], inc[(size_t)a * Vn + i]);
                     om[(size_t)a * Vn + i] = w;
                     bad |= !(isfinite((double)w.x) && isfinite((double)w.y));
@@ -2985,7 +3026,9 @@ struct Engine : EngineBase {
         }
         reduce<3>(Vn, [=] __device__(size_t i, double* acc) {
             bool bad = false;
-            for (int a = 0; a < nm; ++a) {
+#pragma unroll
+            for (int a = 0; a < MAXMODE; ++a) {
+                if (a >= nm) break;
                 V w = om[(size_t)a * Vn + i];
                 w = cadd(w, cscale(u0[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
                 w = cadd(w, cscale(u1[(size_t)a * Vn + i], (T)(co.s[a] * d->dt_scale)));
@@ -3467,7 +3510,9 @@ struct Engine : EngineBase {
         const int nm = c.nm;
         const V* om = which ? omega_bar.p : omega.p;
         reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
-            for (int a = 0; a < nm; ++a) {
+#pragma unroll
+            for (int a = 0; a < MAXMODE; ++a) {
+                if (a >= nm) break;
                 const double2 wd = to_d(om[(size_t)a * Vn + i]);
                 acc[2 * a] += wd.x * wd.x - wd.y * wd.y;
                 acc[2 * a + 1] += 2.0 * wd.x * wd.y;

@@ -1199,31 +1199,6 @@ __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int plane_swz(int z) { return z ^ ((z >> 4) & 7); }
 
-// One-shot bulk copy global -> shared completing on an mbarrier (the TMA
-// unit's untiled copy: both addresses 16-byte aligned, size a multiple of 16).
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void bulk_copy_start(void* sdst, const void* gsrc, unsigned bytes, unsigned long long* mbar)
-{
-    const unsigned b = smem_u32(mbar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes), "r"(b) : "memory");
-}
-// Waits for phase 0 of the mbarrier, at most `tries` polls; false on timeout.
-__device__ __forceinline__ bool bulk_copy_wait(unsigned long long* mbar, int tries)
-{
-    const unsigned b = smem_u32(mbar);
-    for (int k = 0; k < tries; ++k) {
-        unsigned done;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(done) : "r"(b) : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
 // Global loads per point of a pointwise op (Op::LOADS where declared, else 4).
 template <class Op, class = void>
 struct op_loads {
@@ -1260,24 +1235,13 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
     // (t < 8, i < 16): its 16 consecutive threads take 16 consecutive
     // entries, where the plain table would serve them with bank conflicts
     V* stz = stw + N;
-    // rows 0..63 of the plane's class table, copied in by the bulk-copy unit
-    // at kernel start: the table is not written during a sweep, so the copy
-    // goes out before the wait for the previous pass and is in shared memory
-    // by the pointwise step (rows 64..127 are loaded from L2 there)
-    V* se = stz + 128;
-    __shared__ alignas(8) unsigned long long mbar;
-    static_assert(Op::LOADS == 1, "forward segment ops (one load: the class table)");
     const int tid = threadIdx.x;
     const int x = blockIdx.x;
     const int f = blockIdx.y;
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
-    const V* eplane = op.E + base;
-    if (tid == 0) {
-        bulk_copy_start(se, eplane, (unsigned)(sizeof(V) * 64 * N), &mbar);
-        op.prefetch(base + 64 * N, (unsigned)(NE / 2));   // L2 prefetch: cannot observe a stale value
-    }
     for (int j = tid; j < N; j += 1024) stw[j] = twn[j];
     if (tid < 128) stz[tid] = twn[(tid >> 4) * (tid & 15)];
+    if (tid == 0) op.prefetch(base, (unsigned)NE);   // L2 prefetch: cannot observe a stale value
     pdl_wait();
     op.preload();
     const int zc = tid & 127;   // column of the y-stages
@@ -1323,9 +1287,6 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
         __syncthreads();
     }
     op.begin();
-    // every thread polls the barrier (bounded; on a timeout the table rows
-    // are loaded from global memory instead)
-    const bool se_ok = bulk_copy_wait(&mbar, 1 << 20);
     // inverse z, stage 1 (radix 8, span 16) -> op -> forward z, stage 0
     // (radix 8, span 1): butterfly i = tid & 15 of rows yq = tid/16 + 64q
     {
@@ -1351,13 +1312,8 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
             }
             dftR<S1, 8>(u[q]);
             typename Op::Pre pre[8];
-            if (q == 0 && se_ok) {
 #pragma unroll
-                for (int t = 0; t < 8; ++t) pre[t].e = se[y * N + i + 16 * t];
-            } else {
-#pragma unroll
-                for (int t = 0; t < 8; ++t) pre[t] = op.load(f, base + (size_t)y * N + i + 16 * t);
-            }
+            for (int t = 0; t < 8; ++t) pre[t] = op.load(f, base + (size_t)y * N + i + 16 * t);
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
                 const int z = i + 16 * t;
@@ -1412,7 +1368,6 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
             for (int t = 0; t < 8; ++t) dst[base + (size_t)(hi + 8 * q + 16 * t) * N + zc] = u[q][t];
         }
     }
-    if (!se_ok) bulk_copy_wait(&mbar, 1 << 22);   // no copy in flight at exit
     op.end(reinterpret_cast<double*>(tile), blockIdx.x + (size_t)blockIdx.y * gridDim.x);
 }
 
