@@ -2789,6 +2789,18 @@ struct Engine : EngineBase {
             for (int al = 0; al < M; ++al)
                 co.g[a * MAXM + al] = make_double2(c.gamma[a].x * c.O[a * M + al], c.gamma[a].y * c.O[a * M + al]);
         }
+        if (nm == 1 && M == 1) {   // one mode, one monomer type: two accumulators
+            const double c0 = co.c[0];
+            const double2 g0 = co.g[0];
+            reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
+                const V w = om[i];
+                u[i] = cadd(cscale(w, (T)c0), cmul(rt[i], from_d<V>(g0)));
+                const double2 wd = to_d(w);
+                acc[0] += wd.x * wd.x - wd.y * wd.y;
+                acc[1] += 2.0 * wd.x * wd.y;
+            }, ds->fsq, 3.0 * sizeof(V));
+            return;
+        }
         reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
 #pragma unroll
             for (int a = 0; a < MAXMODE; ++a) {
@@ -3509,6 +3521,14 @@ struct Engine : EngineBase {
         const size_t Vn = V_;
         const int nm = c.nm;
         const V* om = which ? omega_bar.p : omega.p;
+        if (nm == 1) {
+            reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
+                const double2 wd = to_d(om[i]);
+                acc[0] += wd.x * wd.x - wd.y * wd.y;
+                acc[1] += 2.0 * wd.x * wd.y;
+            }, ds->fsq);
+            return;
+        }
         reduce<2 * MAXMODE>(Vn, [=] __device__(size_t i, double* acc) {
 #pragma unroll
             for (int a = 0; a < MAXMODE; ++a) {
