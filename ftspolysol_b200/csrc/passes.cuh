@@ -590,7 +590,9 @@ struct OpBond {
     }
     __device__ __forceinline__ V apply(int, int x, int y, int z, size_t g, V v, const Pre& pre)
     {
-        const T phi = phix[x] * phiy[y] * phiz[z];
+        // read-only loads: they do not alias the Fstore writes, so the y and z
+        // factors (fixed for a thread's column) are loaded once
+        const T phi = __ldg(phix + x) * __ldg(phiy + y) * __ldg(phiz + z);
         if (FWD) {
             if (Fstore) Fstore[g] = v;
         } else if (STRESS) {
