@@ -195,7 +195,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
 #pragma unroll
     for (int c = 0; c < K; ++c) acc[c] = 0.0;
     pdl_wait();
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) f(i, acc);
+    // items i, i + stride, ... in that order; U at a time, so that the loads
+    // of U items are in flight together where f's loads cannot alias its
+    // stores (read-only loads); the per-thread summation order is unchanged
+    constexpr int U = K <= 6 ? 4 : 2;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) f(i + u * stride, acc);
+    }
+    for (; i < n; i += stride) f(i, acc);
     pdl_trigger();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -391,10 +401,10 @@ struct SigTab {
 // a[i] for a run-time i < K with constant indices only: an array in a
 // kernel's parameter block indexed at run time is copied to local memory
 // by every thread
-template <int K>
-__device__ __forceinline__ double pick(const double (&a)[K], int i)
+template <typename U, int K>
+__device__ __forceinline__ U pick(const U (&a)[K], int i)
 {
-    double v = a[0];
+    U v = a[0];
 #pragma unroll
     for (int k = 1; k < K; ++k)
         if (i == k) v = a[k];
@@ -480,6 +490,71 @@ struct OpPrecond {
         if (f == dc0 && (x | y | z) == 0) return mkc<cplx<T>>(T(0), T(0));
         return cscale(k, invV);
     }
+    __device__ __forceinline__ void end(double*, size_t) {}
+};
+
+// k-space factors of the density evaluation, applied in the x-pencil pass
+// between the forward and inverse x transforms (the y and z transforms run
+// in the plane passes on either side): output field f is the transform of
+// source field src[f] times c_f F_f(k), F_f the smearing Gamma(k) (lap_f = 0)
+// or k^2 (lap_f = 1), c_f including the 1/V of the unnormalised inverse; the
+// k-space values of the fields f < nst (whose source is f itself) are
+// written to kst, the Fourier fields that the k-space observables read.
+template <typename T>
+struct OpKScale {
+    using V = cplx<T>;
+    static constexpr int NSRC = 4;
+    static constexpr int FUSED_MIN_BLOCKS = 8;
+    V* kst;
+    const T* gm;             // Gamma per axis: x, then y, then z
+    const double* kx;
+    const double* ky;
+    const double* kz;
+    int m1, m2;
+    int nst;
+    int src[NSRC];
+    int lap[NSRC];
+    double2 c[NSRC];
+    struct Pre {};
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ Pre load(int, size_t) const { return Pre{}; }
+    __device__ __forceinline__ V apply(int f, int x, int y, int z, size_t g, V v, const Pre&) const
+    {
+        if (f < nst) kst[g] = v;
+        double fac;
+        if (pick(lap, f)) {
+            const double ax = __ldg(kx + x), ay = __ldg(ky + y), az = __ldg(kz + z);
+            fac = ax * ax + ay * ay + az * az;
+        } else {
+            fac = (double)(__ldg(gm + x) * __ldg(gm + m1 + y) * __ldg(gm + m1 + m2 + z));
+        }
+        return from_d<V>(dscale(dmul(to_d(v), pick(c, f)), fac));
+    }
+    __device__ __forceinline__ void end(double*, size_t) {}
+};
+
+// Loads of the fused density transform (one monomer type): field 0 the
+// monomer density, field 1 the polymer charge density plus zf times the
+// monomer density (the charge of a uniformly charged species, accumulated
+// once here instead of per segment), field 2 the combined ion charge.
+template <typename T>
+struct OpLoadDensity {
+    using V = cplx<T>;
+    const V* rho;            // monomer density, charge density, ion charge
+    size_t Vn;
+    double zf;               // 0: no folded charge
+    struct Pre {
+        V v;
+    };
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ Pre load(int f, size_t g) const
+    {
+        const size_t i = g - (size_t)f * Vn;
+        V a = rho[(size_t)f * Vn + i];
+        if (f == 1 && zf != 0.0) a = cadd(a, cscale(rho[i], (T)zf));
+        return Pre{a};
+    }
+    __device__ __forceinline__ V apply(int, int, int, int, size_t, V, const Pre& p) const { return p.v; }
     __device__ __forceinline__ void end(double*, size_t) {}
 };
 
@@ -1004,7 +1079,7 @@ struct Engine : EngineBase {
         // may run under stream capture, where nothing can be allocated)
         if (c.scheme == FTSP_SCHEME_SI) upart.alloc(2 * (size_t)c.m1 * (nm + 1));
         eta.alloc((size_t)(nm + 1) * Vn);
-        kA.alloc((size_t)(nm + 1) * Vn);
+        kA.alloc((size_t)2 * (nm + 1) * Vn);   // upper half: scratch of the fused evaluation's first pass
         kB.alloc((size_t)(M + 1 + J) * Vn);
         dB.alloc((size_t)(M + 1 + J) * Vn);
         kC.alloc((size_t)(M + 3) * Vn);
@@ -2043,14 +2118,34 @@ struct Engine : EngineBase {
                 return;
             }
         }
-        auto k = k_strided_ct<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
-        set_smem(k, smem);
-        launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, src, dst, (size_t)V_,
-                    (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
-        ++launches;
+        if constexpr (op_has_src<Op>::value) {
+            throw std::runtime_error("pencil op with a source map needs the fused pencil pass");
+        } else {
+            auto k = k_strided_ct<T, N, WCT, DIM, RMAX, NT, E, S1, S2, Op>;
+            set_smem(k, smem);
+            launch_pass(k, dim3(outer * (c.m3 / WCT), nf), NT, smem, c.m2, c.m3, src, dst, (size_t)V_,
+                        (const V*)(DIM == 1 ? tw2.p : tw1.p), op);
+            ++launches;
+        }
     }
 
     bool strided_is_ct(int n) const { return c.m3 % WCT == 0 && (n == 32 || n == 64 || n == 128); }
+
+    // the x pass of length n runs k_strided_fused (both transforms in one pass)
+    template <int N>
+    static constexpr bool x_fused_ct()
+    {
+        constexpr int E = F32 ? 16 : 8;
+        return strided_fused_ok<N, WCT, RMAX, N * WCT / E, E>();
+    }
+    bool x_fused(int n) const
+    {
+        if (!fused_strided || !strided_is_ct(n)) return false;
+        return n == 128 ? x_fused_ct<128>() : n == 64 ? x_fused_ct<64>() : x_fused_ct<32>();
+    }
+    // the density evaluation with its k-space factors inside x-pencil passes:
+    // one interaction mode, one monomer type, every ion smeared like the beads
+    bool eval_fused_ok() const { return plane_ok && c.nm == 1 && c.M == 1 && ion_common && x_fused(c.m1); }
 
     template <int DIM, int S1, int S2, class Op>
     void strided(const V* src, V* dst, int nf, const Op& op)
@@ -2063,14 +2158,18 @@ struct Engine : EngineBase {
                 return strided_ct<DIM, 32, S1, S2>(src, dst, nf, op);
             }
         }
-        const LineGeom& g = DIM == 1 ? gy : gx;
-        auto k = k_strided<T, EL, DIM, S1, S2, Op>;
-        const size_t smem = DIM == 1 ? y_smem : x_smem;
-        set_smem(k, smem);
-        const int outer = DIM == 1 ? c.m1 : c.m2;
-        k<<<dim3(outer * (c.m3 / g.W), nf), DIM == 1 ? y_threads : x_threads, smem, stream>>>(g, src, dst, V_,
-                                                                                            DIM == 1 ? tw2.p : tw1.p, op);
-        ++launches;
+        if constexpr (op_has_src<Op>::value) {
+            throw std::runtime_error("pencil op with a source map needs the fused pencil pass");
+        } else {
+            const LineGeom& g = DIM == 1 ? gy : gx;
+            auto k = k_strided<T, EL, DIM, S1, S2, Op>;
+            const size_t smem = DIM == 1 ? y_smem : x_smem;
+            set_smem(k, smem);
+            const int outer = DIM == 1 ? c.m1 : c.m2;
+            k<<<dim3(outer * (c.m3 / g.W), nf), DIM == 1 ? y_threads : x_threads, smem, stream>>>(g, src, dst, V_,
+                                                                                                DIM == 1 ? tw2.p : tw1.p, op);
+            ++launches;
+        }
     }
 
     template <int S1, int S2, class Op>
@@ -2526,15 +2625,49 @@ struct Engine : EngineBase {
         const V* ps = which ? psi_bar.p : psi.p;
         const int m1 = c.m1, m2 = c.m2, m3 = c.m3;
         const bool elec = c.elec;
+        const bool fx = eval_fused_ok();
+        if (fx) {
+            // 1-2 fused: yz forward of omega and psi (into the scratch half of
+            // kA); one x-pencil pass: x forward, the k-space omega and psi
+            // stored in kA, W_type = gamma O Gamma omega / V, psi_s = Gamma
+            // psi / V and the psi drift's k^2 psi / (4 pi l_B V) (from psi's
+            // transform a second time), x inverse into kB; yz inverse
+            cudaEvent_t ev = prof_begin();
+            V* kAx = kA.p + (size_t)(nm + 1) * Vn;
+            OpLoadN<T> in{};
+            in.s[0] = om;
+            in.s[1] = ps;
+            in.fs = Vn;
+            plane<0, -1>(nullptr, kAx, 2, in);
+            const double invV = 1.0 / (double)Vn;
+            OpKScale<T> op{};
+            op.kst = kA.p;
+            op.gm = gam.p;
+            op.kx = kx.p;
+            op.ky = ky.p;
+            op.kz = kz.p;
+            op.m1 = m1;
+            op.m2 = m2;
+            op.nst = 2;
+            op.src[0] = 0; op.src[1] = 1; op.src[2] = 1; op.src[3] = 3;
+            op.lap[2] = 1;
+            op.c[0] = make_double2(c.gamma[0].x * c.O[0] * invV, c.gamma[0].y * c.O[0] * invV);
+            op.c[1] = make_double2(elec ? invV : 0.0, 0.0);
+            op.c[2] = make_double2(elec ? invV / (4.0 * PI * c.lB) : 0.0, 0.0);
+            strided<0, -1, +1>(kAx, kB.p, 3, op);
+            plane<+1, 0>(kB.p, nullptr, 3, OpStore<T>{kB.p});
+            // plane: 2 in, 2 out; pencil: 3 in, 2 + 3 out; plane: 3 in, 3 out
+            prof_end(ev, "field_fft", 18.0 * sizeof(V) * (double)Vn);
+        }
         // 1. DFT of the mode fields and psi
-        {
+        if (!fx) {
             std::vector<const V*> src;
             for (int a = 0; a < nm; ++a) src.push_back(om + (size_t)a * Vn);
             src.push_back(ps);
             fft3<-1>(kA.p, nm + 1, src.data());
         }
         // 2. k-space: W_type_s (M), psi_s, ion psi_j (J), all scaled by 1/V
-        {
+        if (!fx) {
             GCoef co{};
             for (int a = 0; a < nm; ++a)
                 for (int al = 0; al < M; ++al)
@@ -2566,7 +2699,7 @@ struct Engine : EngineBase {
                 }
             }, (double)(c.nm + 1 + c.M + 1 + Jk) * sizeof(V));
         }
-        fft3<+1>(kB.p, M + 1 + (ion_common ? 0 : J));
+        if (!fx) fft3<+1>(kB.p, M + 1 + (ion_common ? 0 : J));
         // 3. class tables exp(-(W_type + i z psi_s)), ion Boltzmann factors, zeroed accumulators
         {
             ClsTab ct{};
@@ -2584,10 +2717,21 @@ struct Engine : EngineBase {
             if (ion_common) {
                 // the Boltzmann factors exp(-i z_j psi_s) are only summed here
                 // (Q_j); the combined ion charge is formed after the sweeps
+                // class 0 with constant indices (a single class is the usual case)
+                const int t0 = ct.type[0];
+                const T z0 = (T)ct.z[0];
                 reduce<6>(Vn, [=] __device__(size_t i, double* acc) {
-                    const V ps_ = kBp[(size_t)M * Vn + i];
-                    for (int k = 0; k < ncls; ++k) {
-                        V w = kBp[(size_t)ct.type[k] * Vn + i];
+                    const V ps_ = __ldg(kBp + (size_t)M * Vn + i);
+                    {
+                        V w = __ldg(kBp + (size_t)t0 * Vn + i);
+                        if (z0 != T(0)) {
+                            w.x += -(ps_.y * z0);
+                            w.y += ps_.x * z0;
+                        }
+                        Ep[i] = cexpT(-w.x, -w.y);
+                    }
+                    for (int k = 1; k < ncls; ++k) {
+                        V w = __ldg(kBp + (size_t)ct.type[k] * Vn + i);
                         const T zz = (T)ct.z[k];
                         if (zz != T(0)) {
                             w.x += -(ps_.y * zz);
@@ -2639,7 +2783,7 @@ struct Engine : EngineBase {
         if (stress) FTSP_CUDA(cudaMemsetAsync(spart.p, 0, sizeof(double) * 12 * (size_t)x_ctas(), stream));
         // 4. chain propagators of every species
         for (int isp = 0; isp < (int)c.sp.size(); ++isp) solve_species(isp, stress);
-        charge_fold();
+        if (!fx) charge_fold();
         if (ion_common) {
             // the combined ion charge sum_j z_j (n_j/V)/Q_j exp(-i z_j psi_s)
             // (ion_density_from_psi, common.h:1117-1130, summed over the
@@ -2660,8 +2804,40 @@ struct Engine : EngineBase {
             }, 2.0 * sizeof(V));
         }
         const int Jd = ion_common ? 1 : J;   // ion fields of the density transform
+        if (fx) {
+            // 5-7 fused: the raw densities (the folded charge added as the
+            // charge density is loaded) and the combined ion charge, yz
+            // forward (into kC); one x-pencil pass: x forward, their k-space
+            // values stored in dB (the k-space observables read them), times
+            // Gamma / V, x inverse (in place); yz inverse
+            cudaEvent_t ev = prof_begin();
+            OpLoadDensity<T> ld{};
+            ld.rho = dB.p;
+            ld.Vn = Vn;
+            for (size_t k = 0; k < fold_type.size(); ++k)
+                if (fold_type[k] >= 0) ld.zf += fold_z[k];   // one type: at most one species folds
+            plane<0, -1>(nullptr, kC.p, 3, ld);
+            const double invV = 1.0 / (double)Vn;
+            OpKScale<T> op{};
+            op.kst = dB.p;
+            op.gm = gam.p;
+            op.kx = kx.p;
+            op.ky = ky.p;
+            op.kz = kz.p;
+            op.m1 = m1;
+            op.m2 = m2;
+            op.nst = 3;
+            for (int f = 0; f < 4; ++f) {
+                op.src[f] = f;
+                op.c[f] = make_double2(invV, 0.0);
+            }
+            strided<0, -1, +1>(kC.p, kC.p, 3, op);
+            plane<+1, 0>(kC.p, nullptr, 3, OpStore<T>{kC.p});
+            // plane: 3 in, 3 out; pencil: 3 in, 3 + 3 out; plane: 3 in, 3 out
+            prof_end(ev, "field_fft", 21.0 * sizeof(V) * (double)Vn);
+        }
         // 5. DFT of the raw densities and the ion Boltzmann factors (or the combined ion charge)
-        fft3<-1>(dB.p, M + 1 + Jd);
+        if (!fx) fft3<-1>(dB.p, M + 1 + Jd);
         // 6. ion partition functions from the DC bins
         if (J > 0 && !ion_common) {
             DevScal* d = ds;
@@ -2677,7 +2853,7 @@ struct Engine : EngineBase {
             ++launches;
         }
         // 7. k-space: smoothed densities, ion charge, psi drift part
-        {
+        if (!fx) {
             const V* dBp = dB.p;
             const V* kAp = kA.p;
             V* kCp = kC.p;
@@ -2715,7 +2891,7 @@ struct Engine : EngineBase {
                 kCp[(size_t)(M + 2) * Vn + i] = from_d<V>(dscale(to_d(kAp[(size_t)nm * Vn + i]), k2 * invV * dpsi_scale));
             }, (double)(2 * c.M + 5 + Jd) * sizeof(V));
         }
-        fft3<+1>(kC.p, M + 3);
+        if (!fx) fft3<+1>(kC.p, M + 3);
         // 8. real-space epilogue: rho_p, rho_c, ion densities, raw psi drift (+ its sum)
         {
             const V* kCp = kC.p;
@@ -2724,6 +2900,7 @@ struct Engine : EngineBase {
             V* rc = rho_c.p;
             V* ir = ion_rho.p;
             V* dp = which ? dpsi_bar.p : dpsi.p;
+            const V* dk = fx ? kB.p + (size_t)(M + 1) * Vn : kC.p + (size_t)(M + 2) * Vn;   // k^2 psi part
             const DevScal* d = ds;
             IonTab iz{};
             for (int j = 0; j < J; ++j) {
@@ -2733,15 +2910,15 @@ struct Engine : EngineBase {
             const bool common = ion_common;
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
                 V sum = mkc<V>(T(0), T(0));
-                for (int al = 0; al < M; ++al) sum = cadd(sum, kCp[(size_t)al * Vn + i]);
+                for (int al = 0; al < M; ++al) sum = cadd(sum, __ldg(kCp + (size_t)al * Vn + i));
                 rp[i] = sum;
-                const V rcp = kCp[(size_t)M * Vn + i];
-                const V rci = kCp[(size_t)(M + 1) * Vn + i];
+                const V rcp = __ldg(kCp + (size_t)M * Vn + i);
+                const V rci = __ldg(kCp + (size_t)(M + 1) * Vn + i);
                 const V rcv = elec ? cadd(rcp, rci) : mkc<V>(T(0), T(0));
                 rc[i] = rcv;
                 for (int j = 0; j < J; ++j) {
                     if (elec) {
-                        const V pj = kBp[(size_t)(common ? M : M + 1 + j) * Vn + i];
+                        const V pj = __ldg(kBp + (size_t)(common ? M : M + 1 + j) * Vn + i);
                         const T zz = (T)iz.z[j];
                         const V b = cexpT(zz * pj.y, -zz * pj.x);
                         ir[(size_t)j * Vn + i] = cmul(b, from_d<V>(d->ion_factor[j]));
@@ -2749,7 +2926,7 @@ struct Engine : EngineBase {
                         ir[(size_t)j * Vn + i] = mkc<V>((T)iz.nd[j], T(0));
                     }
                 }
-                V dv = kCp[(size_t)(M + 2) * Vn + i];
+                V dv = __ldg(dk + i);
                 if (elec) {
                     dv.x -= rcv.y;   // + i * rho_c
                     dv.y += rcv.x;
@@ -2793,8 +2970,8 @@ struct Engine : EngineBase {
             const double c0 = co.c[0];
             const double2 g0 = co.g[0];
             reduce<2>(Vn, [=] __device__(size_t i, double* acc) {
-                const V w = om[i];
-                u[i] = cadd(cscale(w, (T)c0), cmul(rt[i], from_d<V>(g0)));
+                const V w = __ldg(om + i);
+                u[i] = cadd(cscale(w, (T)c0), cmul(__ldg(rt + i), from_d<V>(g0)));
                 const double2 wd = to_d(w);
                 acc[0] += wd.x * wd.x - wd.y * wd.y;
                 acc[1] += 2.0 * wd.x * wd.y;

@@ -901,6 +901,27 @@ __host__ __device__ constexpr bool strided_fused_ok()
            N * W == NT * E;
 }
 
+// Source field of output field f of a pencil pass: Op::NSRC entries of
+// Op::src where the op declares them (an output computed from another
+// field's transform), else f.  The entries are read with constant indices.
+template <class Op, class = void>
+struct op_has_src : std::false_type {};
+template <class Op>
+struct op_has_src<Op, std::void_t<decltype(Op::NSRC)>> : std::true_type {};
+template <class Op>
+__device__ __forceinline__ int op_src_field(const Op& op, int f)
+{
+    if constexpr (op_has_src<Op>::value) {
+        int s = f;
+#pragma unroll
+        for (int k = 0; k < Op::NSRC; ++k)
+            if (k == f) s = op.src[k];
+        return s;
+    } else {
+        return f;
+    }
+}
+
 template <typename T, int N, int W, int DIM, int RMAX, int NT, int E, int S1, int S2, class Op>
 __global__ void __launch_bounds__(NT, Op::FUSED_MIN_BLOCKS) k_strided_fused(int m2, int m3, const cplx<T>* src, cplx<T>* dst,
                                                          size_t fstride, const cplx<T>* __restrict__ twn, Op op)
@@ -924,7 +945,9 @@ __global__ void __launch_bounds__(NT, Op::FUSED_MIN_BLOCKS) k_strided_fused(int 
     const int f = blockIdx.y;
     const size_t plane = (size_t)m2 * m3;
     const size_t lstride = DIM == 1 ? (size_t)m3 : plane;
-    const size_t base = (size_t)f * fstride + (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
+    const size_t inner = (DIM == 1 ? (size_t)outer * plane : (size_t)outer * m3) + z0;
+    const size_t base = (size_t)f * fstride + inner;
+    const size_t sbase = (size_t)op_src_field(op, f) * fstride + inner;
     for (int j = threadIdx.x; j < N; j += NT) stw[j] = twn[j];
     pdl_wait();
     // load: value u of the thread is position tid/W + u*NT/W of column tid%W
@@ -932,7 +955,7 @@ __global__ void __launch_bounds__(NT, Op::FUSED_MIN_BLOCKS) k_strided_fused(int 
 #pragma unroll
     for (int u = 0; u < E; ++u) {
         const int e = threadIdx.x + u * NT;
-        v[u] = src[base + (e / W) * lstride + e % W];
+        v[u] = src[sbase + (e / W) * lstride + e % W];
     }
     __syncthreads();   // twiddles in shared memory
     {
