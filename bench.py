@@ -66,6 +66,8 @@ def parse_args():
                     help="device checkpoint interval of the time-to-Pi runs (the reference's Ntmp)")
     ap.add_argument("--ttp-max-restarts", type=int, default=1000,
                     help="rollbacks allowed in a time-to-Pi run (the reference's max_nan_restarts)")
+    ap.add_argument("--ttp-seed-runs", type=int, default=0,
+                    help="extra complex128 runs at the target step with other noise seeds (spread of the target)")
     ap.add_argument("--ttp-train-steps", type=int, default=2000,
                     help="plain semi-implicit steps whose statistics train the network")
     ap.add_argument("--replicas", type=int, default=0,
@@ -717,8 +719,8 @@ def run_time_to_pi(args, local):
 
     every, cap = args.ttp_checkpoint_every, args.ttp_max_restarts
 
-    def engine(prec, dt):
-        e = Engine(dict(d, dt=dt), precision=prec, scheme=SCHEME_SI, noise=True, seed=21, device=local,
+    def engine(prec, dt, seed=21):
+        e = Engine(dict(d, dt=dt), precision=prec, scheme=SCHEME_SI, noise=True, seed=seed, device=local,
                    restart_interval=every, max_restarts=cap)
         e.set_fields(om, ps)
         if args.adaptive > 0:
@@ -726,8 +728,8 @@ def run_time_to_pi(args, local):
         torch.cuda.synchronize()
         return e
 
-    def plain(prec, dt, tag):
-        e = engine(prec, dt)
+    def plain(prec, dt, tag, seed=21):
+        e = engine(prec, dt, seed)
         tr = _Trajectory(e, every, idx, time.perf_counter(), args.adaptive > 0)
         limit = 4 * int(round(T / dt))   # step attempts, rolled-back ones included
         while tr.sim < T - 0.5 * dt and not tr.stopped and tr.attempts < limit:
@@ -773,6 +775,10 @@ def run_time_to_pi(args, local):
     target = (_wmean(half, 2), _wmean(half, 3), _wmean(half, 4))
     bm = np.array([[_wmean(b, c) for c in (2, 3, 4)] for b in np.array_split(half, 10)])
     target_se = bm.std(axis=0, ddof=1) / np.sqrt(len(bm))
+    # the target step with other noise seeds: how far apart independent
+    # trajectories of the same length land (the resolution of the criterion)
+    for k in range(args.ttp_seed_runs):
+        plain(FP64, 0.005, "c128_si_dt0.005_seed%d" % (22 + k), seed=22 + k)
     plain(FP32, 0.005, "c64_si_dt0.005")
     for dt in args.ttp_dts:
         plain(FP32, dt, "c64_si_dt%g" % dt)
@@ -810,6 +816,8 @@ def run_time_to_pi(args, local):
                       "speedup_vs_c128": (base / best[1]) if (base and best) else None,
                       "Pi_alone": {"time_to_1pct_s": pi_only, "best_learned_run": best_pi[1] if best_pi else None,
                                    "speedup_vs_c128": (base_pi / best_pi[0]) if (base_pi and best_pi) else None},
+                      "seed_spread": {tag: {"Pi_rel_err": v.get("Pi_rel_err"), "mu_rel_err": v.get("mu_rel_err")}
+                                      for tag, v in out.items() if tag.startswith("c128_si_dt0.005_seed")},
                       "target": {"Pi": target[0], "mu": target[1], "mu_ex": target[2],
                                  "Pi_se": float(target_se[0]), "mu_se": float(target_se[1]),
                                  "mu_ex_se": float(target_se[2])},
