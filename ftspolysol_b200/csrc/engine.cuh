@@ -2051,7 +2051,8 @@ struct Engine : EngineBase {
         if constexpr (S1 != 0 && S2 != 0 && F32 && N == 128 && NT == 1024 && op_loads<Op>::value <= 1) {
             if (zreg_plane) {
                 auto k = k_plane_zreg<T, S1, S2, Op>;
-                const size_t zsmem = smem + sizeof(V) * 128;   // + the [t][i] twiddle table
+                // tile of 128 x ZREG_P values, the twiddles, the [t][i] and [t][b] twiddle tables
+                const size_t zsmem = sizeof(V) * ((size_t)128 * ZREG_P + 128 + 128 + 128);
                 set_smem(k, zsmem);
                 launch_pass(k, dim3(c.m1, nf), NT, zsmem, src, dst, (size_t)V_, (const V*)tw3.p, op);
                 ++launches;

@@ -1214,15 +1214,21 @@ __global__ void __launch_bounds__(NT, 2) k_zline_ct(int m2, const cplx<T>* src, 
 // (the op's loads and stores are coalesced).  The forward stage writes
 // positions 8i + t, a stride of 8 complex values; the tile's z index is
 // swizzled, z ^ ((z >> 4) & 7), which keeps every half-warp access of every
-// stage on 16 distinct 8-byte bank slots (rows are padded to 129 values, so
-// accesses along y are spread by the row as well).
+// stage on 16 distinct 8-byte bank slots (rows are padded to ZREG_P values).
+// Every z stage works on rows that one warp owns, so the z phase needs no
+// block-wide barrier.
 //
 // Shared-memory round trips: 6 (y: 2, z: 2, z: 2 less the fused pair, y: 2
-// less the register-resident first and last stages); barriers: 11.  Same
-// grid, Op interface (forward ops: one load per point) and results, up to
-// the rounding of the operation order, as k_plane_fused.
+// less the register-resident first and last stages); block barriers: 7.
+// Same grid, Op interface (forward ops: one load per point) and results, up
+// to the rounding of the operation order, as k_plane_fused.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int plane_swz(int z) { return z ^ ((z >> 4) & 7); }
+
+// Row pitch of the k_plane_zreg tile: 136 values (272 banks = 16 mod 32), so
+// the two rows of a half-warp in the warp-owned z stages fall on opposite
+// halves of the banks; accesses along y keep one row per half-warp.
+constexpr int ZREG_P = 136;
 
 // Global loads per point of a pointwise op (Op::LOADS where declared, else 4).
 template <class Op, class = void>
@@ -1251,7 +1257,7 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
                                                         const cplx<T>* __restrict__ twn, Op op)
 {
     using V = cplx<T>;
-    constexpr int N = 128, P = N + 1, NE = N * N;
+    constexpr int N = 128, P = ZREG_P, NE = N * N;
     static_assert(S1 != 0 && S2 != 0, "both transforms");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
@@ -1260,12 +1266,16 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
     // (t < 8, i < 16): its 16 consecutive threads take 16 consecutive
     // entries, where the plain table would serve them with bank conflicts
     V* stz = stw + N;
+    // twiddles w^(t b) of the warp-owned radix-16 z stage laid out [t][b]
+    // (t < 16, b < 8): the 8 butterflies of a row read consecutive entries
+    V* stb = stz + 128;
     const int tid = threadIdx.x;
     const int x = blockIdx.x;
     const int f = blockIdx.y;
     const size_t base = (size_t)f * fstride + (size_t)x * NE;
     for (int j = tid; j < N; j += 1024) stw[j] = twn[j];
     if (tid < 128) stz[tid] = twn[(tid >> 4) * (tid & 15)];
+    else if (tid < 256) stb[tid - 128] = twn[((tid - 128) >> 3) * (tid & 7)];
     if (tid == 0) op.prefetch(base, (unsigned)NE);   // L2 prefetch: cannot observe a stale value
     pdl_wait();
     op.preload();
@@ -1299,34 +1309,39 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
         }
         __syncthreads();
     }
-    // inverse z, stage 0 (radix 16, span 1): row zc (line-fastest), butterfly hi
+    // The z stages run on rows owned by one warp (rows 4w .. 4w+3 of warp
+    // w), so they synchronise with __syncwarp only: the warps drift apart
+    // there, and one warp's global loads of the pointwise step overlap the
+    // transforms and shared-memory exchanges of the others.
+    // inverse z, stage 0 (radix 16, span 1): row 4w + lane / 8, butterfly lane % 8
     {
-        const int y = zc;
+        const int y = 4 * (threadIdx.x >> 5) + ((threadIdx.x & 31) >> 3), b = threadIdx.x & 7;
         V u[16];
 #pragma unroll
-        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(hi + 8 * t)];
-        __syncthreads();
+        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(b + 8 * t)];
+        __syncwarp();
         dftR<S1, 16>(u);
 #pragma unroll
-        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(16 * hi + t)] = u[t];
-        __syncthreads();
+        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(16 * b + t)] = u[t];
+        __syncwarp();
     }
     op.begin();
     // inverse z, stage 1 (radix 8, span 16) -> op -> forward z, stage 0
-    // (radix 8, span 1): butterfly i = tid & 15 of rows yq = tid/16 + 64q
+    // (radix 8, span 1): butterfly i = lane % 16 of rows 4w + (lane / 16) + 2q
     {
-        const int i = tid & 15;
+        const int i = threadIdx.x & 15;
+        const int y0 = 4 * (threadIdx.x >> 5) + ((threadIdx.x >> 4) & 1);   // rows y0 and y0 + 2
         V u[2][8];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int y = (tid >> 4) + 64 * q;
+            const int y = y0 + 2 * q;
 #pragma unroll
             for (int t = 0; t < 8; ++t) u[q][t] = tile[y * P + plane_swz(i + 16 * t)];
         }
-        __syncthreads();
+        __syncwarp();
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int y = (tid >> 4) + 64 * q;
+            const int y = y0 + 2 * q;
             if (i) {
 #pragma unroll
                 for (int t = 1; t < 8; ++t) {
@@ -1348,23 +1363,27 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
         pdl_trigger();
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int y = (tid >> 4) + 64 * q;
+            const int y = y0 + 2 * q;
             dftR<S2, 8>(u[q]);
 #pragma unroll
             for (int t = 0; t < 8; ++t) tile[y * P + plane_swz(8 * i + t)] = u[q][t];
         }
-        __syncthreads();
+        __syncwarp();
     }
-    // forward z, stage 1 (radix 16, span 8): row zc, butterfly hi
+    // forward z, stage 1 (radix 16, span 8): row 4w + lane / 8, butterfly lane % 8
     {
-        const int y = zc;
+        const int y = 4 * (threadIdx.x >> 5) + ((threadIdx.x & 31) >> 3), b = threadIdx.x & 7;
         V u[16];
 #pragma unroll
-        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(hi + 8 * t)];
-        __syncthreads();
-        bfly_k<S2, 16>(u, hi, stw);
+        for (int t = 0; t < 16; ++t) u[t] = tile[y * P + plane_swz(b + 8 * t)];
+        __syncwarp();
+        if (b) {
 #pragma unroll
-        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(hi + 8 * t)] = u[t];
+            for (int t = 1; t < 16; ++t) u[t] = cmul(u[t], twiddle<S2>(stb, t * 8 + b));
+        }
+        dftR<S2, 16>(u);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(b + 8 * t)] = u[t];
         __syncthreads();
     }
     // forward y, stage 0 (radix 16, span 1): column zc, butterfly hi
