@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) k_pair_density_vec(size_t n, PairTable tb
             double sx[PT], sy[PT];
 #pragma unroll
             for (int k = 0; k < PT; ++k) sx[k] = sy[k] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
             for (int j = R.j0; j < R.j1; ++j) {
                 const int2 pr = sp[j];
                 V us[PT], up[PT];
