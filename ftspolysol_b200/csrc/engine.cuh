@@ -375,14 +375,20 @@ __device__ __forceinline__ U4 philox(U4 c, uint32_t k0, uint32_t k1)
     }
     return c;
 }
-// One standard normal per (element, field, step) by the Box-Muller transform
-// of two 53-bit uniforms in (0, 1).
-__device__ __forceinline__ double normal_at(uint64_t seed, uint64_t step, uint32_t field, uint64_t i)
+// Two independent standard normals per (element, field pair, step): the
+// Box-Muller transform of two 53-bit uniforms in (0, 1), both of its outputs
+// (r cos 2 pi u2 for field 2p, r sin 2 pi u2 for field 2p + 1).
+__device__ __forceinline__ void normal_pair_at(uint64_t seed, uint64_t step, uint32_t pair, uint64_t i, double& n0,
+                                               double& n1)
 {
-    const U4 r = philox(U4{(uint32_t)i, (uint32_t)(i >> 32), (uint32_t)step, field}, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const U4 r = philox(U4{(uint32_t)i, (uint32_t)(i >> 32), (uint32_t)step, pair}, (uint32_t)seed, (uint32_t)(seed >> 32));
     const double u1 = ((double)(((uint64_t)r.x << 21) ^ (r.y >> 11)) + 0.5) * (1.0 / 9007199254740992.0);
     const double u2 = ((double)(((uint64_t)r.z << 21) ^ (r.w >> 11)) + 0.5) * (1.0 / 9007199254740992.0);
-    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    n0 = rad * cs;
+    n1 = rad * sn;
 }
 
 // ---- plain-data tables captured by the kernels' lambdas ----
@@ -3017,12 +3023,21 @@ struct Engine : EngineBase {
             // the predictor, remove_real_mean, complexLangevin.cu:296)
             reduce<1>(Vn, [=] __device__(size_t i, double* acc) {
                 const uint64_t st = d->step;
+                const double sc = sqrt(d->dt_scale);
 #pragma unroll
-                for (int f = 0; f <= MAXMODE; ++f) {
+                for (int f = 0; f <= MAXMODE; f += 2) {   // fields f and f + 1 from one draw
                     if (f > nm) break;
-                    const T v = sg.s[f] != 0.0 ? (T)((sg.s[f] * sqrt(d->dt_scale)) * normal_at(seed, st, (uint32_t)f, i)) : T(0);
-                    e[(size_t)f * Vn + i] = v;
-                    if (f == nm) acc[0] += (double)v;
+                    double n0, n1;
+                    normal_pair_at(seed, st, (uint32_t)(f >> 1), i, n0, n1);
+                    const T v0 = sg.s[f] != 0.0 ? (T)((sg.s[f] * sc) * n0) : T(0);
+                    e[(size_t)f * Vn + i] = v0;
+                    if (f == nm) acc[0] += (double)v0;
+                    if (f + 1 <= nm) {
+                        const double s1 = f + 1 <= MAXMODE ? sg.s[f + 1] : 0.0;
+                        const T v1 = s1 != 0.0 ? (T)((s1 * sc) * n1) : T(0);
+                        e[(size_t)(f + 1) * Vn + i] = v1;
+                        if (f + 1 == nm) acc[0] += (double)v1;
+                    }
                 }
             }, &ds->mean_eta, (double)(c.nm + 1) * sizeof(T));
         } else if (c.elec) {   // injected noise: remove_real_mean of its psi part (complexLangevin.cu:296)

@@ -6,15 +6,17 @@ sigma^2 = 2 lambda dt / dV for each interaction mode and for psi
 common.h:300-303, generateNoiseKernel, common.h:582-590) and removes the mean
 of the psi noise (remove_real_mean, complexLangevin.cu:296).  The engine
 draws the same distribution from a counter-based Philox4x32-10 generator
-keyed by (seed, step, field, point) with a Box-Muller transform.  Checked
-here over several steps of a 32^3 system, for both precisions:
+keyed by (seed, step, field pair, point), whose two Box-Muller outputs are
+the noise of the two fields of the pair.  Checked here over several steps
+of a 32^3 system, for both precisions:
 
   * mean and variance of every field against 0 and sigma^2, within 5
     standard errors (the variance of a sample variance is 2 sigma^4 / n);
   * the excess kurtosis against 0 (a Gaussian; standard error sqrt(24/n));
   * the psi noise has zero mean after the removal (to rounding);
   * no correlation between consecutive steps, nor between the mode and psi
-    noise of one step (|r| < 5 / sqrt(n));
+    noise of one step, nor between their squares (the two outputs of one
+    Box-Muller draw are independent, not only uncorrelated) (|r| < 5 / sqrt(n));
   * the same seed reproduces the noise exactly, another seed does not.
 """
 import numpy as np
@@ -76,6 +78,7 @@ def test_noise_moments(prec):
             assert abs(corr(eta[s, f], eta[s + 1, f])) < bound
     for s in range(STEPS):
         assert abs(corr(eta[s, 0], eta[s, 1])) < bound
+        assert abs(corr(eta[s, 0] ** 2, eta[s, 1] ** 2)) < bound
 
 
 def test_noise_seeded():
