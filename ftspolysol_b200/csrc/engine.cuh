@@ -35,7 +35,7 @@ constexpr int MAXSP = 16;
 constexpr int MAXION = 16;
 constexpr int MAXM = 8;
 constexpr int MAXMODE = 8;
-constexpr int RED_BLOCKS = 1184;  // fixed reduction grid (8 x 148 SMs) => deterministic sums
+constexpr int RED_BLOCKS = 1184;  // largest reduction grid (8 x 148 SMs); a kernel's grid is fixed per device => deterministic sums
 constexpr int RED_THREADS = 256;
 constexpr double PI = 3.141592653589793238462643383279502884;
 
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(size_t n, F f, double* p
     // items i, i + stride, ... in that order; U at a time, so that the loads
     // of U items are in flight together where f's loads cannot alias its
     // stores (read-only loads); the per-thread summation order is unchanged
-    constexpr int U = K <= 6 ? 4 : 2;
+    constexpr int U = K <= 6 ? 4 : 1;   // many channels: registers for occupancy instead
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     for (; i + (U - 1) * stride < n; i += U * stride) {
@@ -2003,8 +2003,21 @@ struct Engine : EngineBase {
     void reduce(size_t n, F f, double* out, double bpe = 0.0)
     {
         cudaEvent_t ev = bpe > 0.0 ? prof_begin() : nullptr;
-        launch_pass(k_reduce<K, MAX, F>, dim3(RED_BLOCKS), RED_THREADS, 0, n, f, (double*)part.p);
-        launch_pass(k_combine<MAX>, dim3(K), COMBINE_THREADS, 0, (const double*)part.p, (int)RED_BLOCKS, (int)K, out);
+        // one wave: as many blocks as are resident at once on this device (the
+        // kernel's registers decide), at most RED_BLOCKS; fixed per kernel and
+        // device, so the summation order is too
+        static int grid_of[64] = {};
+        int dev = 0;
+        FTSP_CUDA(cudaGetDevice(&dev));
+        int& grid = grid_of[dev & 63];
+        if (grid == 0) {
+            int per_sm = 0, sms = 0;
+            FTSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_reduce<K, MAX, F>, RED_THREADS, 0));
+            FTSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            grid = std::max(1, std::min(RED_BLOCKS, per_sm * sms));
+        }
+        launch_pass(k_reduce<K, MAX, F>, dim3(grid), RED_THREADS, 0, n, f, (double*)part.p);
+        launch_pass(k_combine<MAX>, dim3(K), COMBINE_THREADS, 0, (const double*)part.p, grid, (int)K, out);
         launches += 2;
         prof_end(ev, "field_reduce", bpe * (double)n);
     }
