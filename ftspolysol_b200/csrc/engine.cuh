@@ -1998,6 +1998,19 @@ struct Engine : EngineBase {
         prof_end(ev, "field_elementwise", bpe * (double)n);
     }
 
+    // Blocks of kernel k resident at once on the current device (one wave),
+    // at most RED_BLOCKS.
+    template <class Kern>
+    static int wave_blocks(Kern k, int threads, size_t smem)
+    {
+        int per_sm = 0, dev = 0, sms = 0;
+        FTSP_CUDA(cudaGetDevice(&dev));
+        FTSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+        FTSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (per_sm <= 0 || sms <= 0) return RED_BLOCKS;   // no answer: the largest grid
+        return std::min(RED_BLOCKS, per_sm * sms);
+    }
+
     // Reduce K channels over n items into out[0..K) (device memory).
     template <int K, bool MAX = false, class F>
     void reduce(size_t n, F f, double* out, double bpe = 0.0)
@@ -2010,12 +2023,7 @@ struct Engine : EngineBase {
         int dev = 0;
         FTSP_CUDA(cudaGetDevice(&dev));
         int& grid = grid_of[dev & 63];
-        if (grid == 0) {
-            int per_sm = 0, sms = 0;
-            FTSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_reduce<K, MAX, F>, RED_THREADS, 0));
-            FTSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            grid = std::max(1, std::min(RED_BLOCKS, per_sm * sms));
-        }
+        if (grid == 0) grid = wave_blocks(k_reduce<K, MAX, F>, RED_THREADS, 0);
         launch_pass(k_reduce<K, MAX, F>, dim3(grid), RED_THREADS, 0, n, f, (double*)part.p);
         launch_pass(k_combine<MAX>, dim3(K), COMBINE_THREADS, 0, (const double*)part.p, grid, (int)K, out);
         launches += 2;
