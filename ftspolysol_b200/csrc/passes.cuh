@@ -1325,48 +1325,51 @@ __global__ void __launch_bounds__(1024, 1) k_plane_zreg(const cplx<T>* src, cplx
         for (int t = 0; t < 16; ++t) tile[y * P + plane_swz(16 * b + t)] = u[t];
         __syncwarp();
     }
-    op.begin();
     // inverse z, stage 1 (radix 8, span 16) -> op -> forward z, stage 0
-    // (radix 8, span 1): butterfly i = lane % 16 of rows 4w + (lane / 16) + 2q
+    // (radix 8, span 1): butterfly i = lane % 16 of rows 4w + (lane / 16) + 2q.
+    // The op's loads depend on neither transform: those of row y0 are issued
+    // before the block reduction of begin() and those of row y0 + 2 right after
+    // the op of row y0, so their latency overlaps the barriers and the
+    // transforms.  Each row is read, transformed, passed through the op and
+    // written back in turn; per value the operations and their order are
+    // those of the two-row form.
+    const int i = threadIdx.x & 15;
+    const int y0 = 4 * (threadIdx.x >> 5) + ((threadIdx.x >> 4) & 1);   // rows y0 and y0 + 2
+    typename Op::Pre pre0[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) pre0[t] = op.load(f, base + (size_t)y0 * N + i + 16 * t);
+    op.begin();
     {
-        const int i = threadIdx.x & 15;
-        const int y0 = 4 * (threadIdx.x >> 5) + ((threadIdx.x >> 4) & 1);   // rows y0 and y0 + 2
-        V u[2][8];
+        typename Op::Pre pre1[8];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int y = y0 + 2 * q;
+            V u[8];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) u[q][t] = tile[y * P + plane_swz(i + 16 * t)];
-        }
-        __syncwarp();
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int y = y0 + 2 * q;
+            for (int t = 0; t < 8; ++t) u[t] = tile[y * P + plane_swz(i + 16 * t)];
+            __syncwarp();   // the row's reads done before its positions are rewritten
             if (i) {
 #pragma unroll
                 for (int t = 1; t < 8; ++t) {
                     V w = stz[t * 16 + i];
                     if (S1 > 0) w.y = -w.y;
-                    u[q][t] = cmul(u[q][t], w);
+                    u[t] = cmul(u[t], w);
                 }
             }
-            dftR<S1, 8>(u[q]);
-            typename Op::Pre pre[8];
-#pragma unroll
-            for (int t = 0; t < 8; ++t) pre[t] = op.load(f, base + (size_t)y * N + i + 16 * t);
+            dftR<S1, 8>(u);
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
                 const int z = i + 16 * t;
-                u[q][t] = op.apply(f, x, y, z, base + (size_t)y * N + z, u[q][t], pre[t]);
+                u[t] = op.apply(f, x, y, z, base + (size_t)y * N + z, u[t], q == 0 ? pre0[t] : pre1[t]);
             }
-        }
-        pdl_trigger();
+            if (q == 0) {
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int y = y0 + 2 * q;
-            dftR<S2, 8>(u[q]);
+                for (int t = 0; t < 8; ++t) pre1[t] = op.load(f, base + (size_t)(y0 + 2) * N + i + 16 * t);
+            }
+            if (q == 1) pdl_trigger();
+            dftR<S2, 8>(u);
 #pragma unroll
-            for (int t = 0; t < 8; ++t) tile[y * P + plane_swz(8 * i + t)] = u[q][t];
+            for (int t = 0; t < 8; ++t) tile[y * P + plane_swz(8 * i + t)] = u[t];
         }
         __syncwarp();
     }
